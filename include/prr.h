@@ -1,0 +1,241 @@
+/*
+ * prr.h -- C ABI of the B200 ProRes RAW decode / linearize / develop library
+ * (libprr.so, CUDA sm_100a).
+ *
+ * The entry points mirror the public API of the proresraw_rs crate
+ * (src/lib.rs:50-66). Each declaration names the crate item it replaces.
+ * Conventions:
+ *  - every call returns an int status: 0 = PRR_OK, negative values map 1:1
+ *    onto the crate's `Error` variants (src/error.rs:6-63), plus library
+ *    statuses (PRR_ERR_BUFFER replaces the crate's panics on wrongly sized
+ *    `_into` buffers);
+ *  - tiles with an invalid header are not errors: they are skipped, their
+ *    sensels written as 0, and listed in frame order (src/decoder.rs:238-245);
+ *  - packets are borrowed; device outputs are caller-owned buffers;
+ *  - a context binds one device and one CUDA stream; calls on one context
+ *    are not thread-safe, calls on different contexts are.
+ * Device-resident inputs must be readable for prr_padded_packet_bytes(len)
+ * bytes and 4-byte aligned (the stream reader loads aligned 32-bit words).
+ */
+#ifndef PRR_H
+#define PRR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PRR_ABI_VERSION 1
+
+enum prr_status {
+    PRR_OK = 0,
+    /* src/error.rs:6-63, in declaration order */
+    PRR_ERR_TRUNCATED = -1,
+    PRR_ERR_FRAME_SIZE_MISMATCH = -2,
+    PRR_ERR_BAD_QUANT_MATRIX = -3,
+    PRR_ERR_BAD_CURVE = -4,
+    PRR_ERR_UNEXPECTED_CURVE = -5,
+    PRR_ERR_BAD_TAG = -6,
+    PRR_ERR_HEADER_TOO_SHORT = -7,
+    PRR_ERR_UNSUPPORTED_VERSION = -8,
+    PRR_ERR_BAD_DIMENSIONS = -9,
+    PRR_ERR_BAD_ALIGNMENT = -10,
+    PRR_ERR_TILE_OUT_OF_BOUNDS = -11,
+    PRR_ERR_BAD_TILE_HEADER = -12,
+    /* library statuses */
+    PRR_ERR_BUFFER = -20,  /* an output buffer has the wrong size (the crate panics) */
+    PRR_ERR_CUDA = -21,    /* a CUDA call failed; see prr_last_error_string */
+    PRR_ERR_TIMEOUT = -22, /* a bounded device loop gave up; the context stays usable */
+    PRR_ERR_INVALID = -23, /* an argument is out of range */
+    PRR_ERR_NO_MEMORY = -24,
+};
+
+/* Payload of an error: the fields of the matching `Error` variant. */
+typedef struct prr_error {
+    int32_t code;
+    char what[32];       /* Truncated::what */
+    uint64_t needed;     /* Truncated::needed */
+    uint64_t available;  /* Truncated::available */
+    uint32_t declared;   /* FrameSizeMismatch::declared */
+    uint64_t actual;     /* FrameSizeMismatch::actual */
+    uint64_t index;      /* BadQuantMatrix::index; TileOutOfBounds::tile; BadTileHeader::tile */
+    uint32_t value;      /* BadQuantMatrix::value; UnsupportedVersion; BadAlignment; HeaderTooShort */
+    uint16_t width, height; /* BadDimensions */
+    uint16_t curve[8];   /* BadCurve */
+    uint8_t tag[4];      /* BadTag */
+} prr_error;
+
+/* FrameHeader, src/header.rs:112-146. */
+typedef struct prr_header {
+    uint8_t version;
+    uint8_t vendor[4];
+    uint8_t bayer_pattern; /* header code: 0 RGGB, 1 GRBG, 2 GBRG, 3 BGGR */
+    uint16_t width, height;
+    uint8_t crop[4]; /* left, right, top, bottom */
+    uint16_t white_level;
+    uint16_t wb_cct;
+    uint16_t flags;
+    uint8_t alignment;
+    uint8_t pad0;
+    float wb_red, wb_blue;
+    float color_matrix[9]; /* row-major camera RGB -> XYZ */
+    float gain;
+    uint8_t quant_matrix[64];
+    uint16_t curve[8];
+} prr_header;
+
+/* Header plus tile grid: the host half of parse_frame (src/decoder.rs:76-123). */
+typedef struct prr_frame_info {
+    prr_header header;
+    uint64_t packet_len;
+    uint64_t table_offset; /* byte offset of the tile size table */
+    uint32_t ntiles, tiles_per_row, tile_rows;
+    uint32_t coded_width, coded_height;
+    uint32_t pad0;
+} prr_frame_info;
+
+/* DemosaicParams, src/demosaic.rs:57-74. */
+typedef struct prr_params {
+    int32_t cfa_phase;
+    int32_t black;
+    float one_over_range;
+    float noise[3];
+    float clip[2];
+    float black_over_range;
+    float wb[2];
+} prr_params;
+
+/* Results of a synchronous decode: Frame / RgbFrame metadata
+ * (src/decoder.rs:132-145, src/reduced.rs:76-94). */
+typedef struct prr_decode_result {
+    prr_header header;
+    uint64_t n_skipped;   /* number of skipped tiles */
+    uint64_t* skipped;    /* caller array, frame order, first skipped_cap entries */
+    uint64_t skipped_cap;
+    uint8_t max_qscale;
+    uint8_t pad[7];
+} prr_decode_result;
+
+/* Status written on the device by the asynchronous decode entry points. */
+typedef struct prr_dev_status {
+    uint32_t oob_tile;   /* first tile whose size-table entry reaches past the packet, or 0xFFFFFFFF */
+    uint32_t n_skipped;  /* tiles skipped for an invalid header */
+    uint32_t max_qscale; /* ParsedFrame::max_qscale */
+    uint32_t error;      /* nonzero when a bounded device loop gave up */
+} prr_dev_status;
+
+enum prr_idct { PRR_IDCT_APPLE = 0, PRR_IDCT_FFMPEG = 1 };             /* src/idct.rs:20-26 */
+enum prr_scale { PRR_SCALE_HALF = 1, PRR_SCALE_QUARTER = 2, PRR_SCALE_EIGHTH = 3 }; /* src/reduced.rs:25-32, value = log2 factor */
+enum prr_greens { PRR_GREENS_FIRST = 0, PRR_GREENS_AVERAGE = 1 };      /* src/reduced.rs:65-72 */
+enum prr_stage { PRR_STAGE_DEMOSAICED = 0, PRR_STAGE_WHITE_BALANCED = 1, PRR_STAGE_REC2020 = 2 }; /* src/demosaic.rs:112-123 */
+enum prr_exposure { PRR_EXPOSURE_NORMALIZED = 0, PRR_EXPOSURE_REFLECTION = 1 }; /* src/demosaic.rs:127-133 */
+enum prr_layout { PRR_INTERLEAVED = 0, PRR_PLANAR = 1 };
+
+typedef struct prr_ctx prr_ctx;
+
+/* --- context ------------------------------------------------------------------ */
+/* One device and one CUDA stream (NULL: the context creates its own). */
+int prr_ctx_create(int device, void* cuda_stream, prr_ctx** out);
+void prr_ctx_destroy(prr_ctx* ctx);
+/* The stream the context enqueues on (a cudaStream_t). */
+void* prr_ctx_stream(prr_ctx* ctx);
+/* Wait for all work enqueued on the context's stream. */
+int prr_sync(prr_ctx* ctx);
+const char* prr_status_string(int status);
+/* Text of the last CUDA error seen by the context (or "" ). */
+const char* prr_last_error_string(prr_ctx* ctx);
+/* Bytes a device packet buffer must provide for a packet of `len` bytes. */
+size_t prr_padded_packet_bytes(size_t len);
+/* Counter of kernel launches made through this library (all contexts). */
+uint64_t prr_kernel_launches(void);
+
+/* --- host-side parsing -------------------------------------------------------- */
+/* header_len, src/decoder.rs:58-73 */
+int prr_header_len(const uint8_t* packet, size_t len, size_t* out, prr_error* err);
+/* parse_header, src/decoder.rs:45-53 */
+int prr_parse_header(const uint8_t* packet, size_t len, prr_header* out, prr_error* err);
+/* parse_frame, src/decoder.rs:76-123, host half: prefix, header and size
+ * table bounds; the per-tile walk (offsets, TileOutOfBounds, max_qscale)
+ * runs on the device during decode. */
+int prr_frame_info_parse(const uint8_t* packet, size_t len, prr_frame_info* out, prr_error* err);
+/* parse_frame, src/decoder.rs:76-123, complete on the host: also walks the
+ * size table for TileOutOfBounds and max_qscale (frame_quantizer,
+ * src/demosaic.rs:50-52). */
+int prr_parse_frame(const uint8_t* packet, size_t len, prr_frame_info* out, uint8_t* max_qscale,
+                    prr_error* err);
+
+/* --- decode (synchronous; packet in host memory) ----------------------------- */
+/* decode_frame / decode_frame_with, src/decoder.rs:221-267. `dev_samples`
+ * is a device buffer of coded_width * coded_height u16 (Frame::samples). */
+int prr_decode(prr_ctx* ctx, const uint8_t* packet, size_t len, int idct, uint16_t* dev_samples,
+               size_t samples_len, prr_decode_result* res, prr_error* err);
+/* decode_frame_reduced / _with, src/reduced.rs:142-201. `dev_rgb` holds
+ * 3 * (coded_width >> s) * (coded_height >> s) u16 (RgbFrame::samples). */
+int prr_decode_reduced(prr_ctx* ctx, const uint8_t* packet, size_t len, int scale, int greens,
+                       uint16_t* dev_rgb, size_t rgb_len, prr_decode_result* res, prr_error* err);
+
+/* --- decode (asynchronous; packet resident on the device) -------------------- */
+/* Device scratch bytes the asynchronous decodes need for a frame. */
+size_t prr_decode_scratch_bytes(const prr_frame_info* info);
+/* Enqueue the decode of `info` (from prr_frame_info_parse) whose bytes are
+ * at `dev_packet`; writes code values (mode full) or linear RGB (reduced),
+ * a prr_dev_status and the skipped tile indices (unordered, up to ntiles)
+ * to device memory. No synchronization, no allocation: suitable for CUDA
+ * graph capture. `dev_scratch` holds prr_decode_scratch_bytes(info) bytes. */
+int prr_decode_async(prr_ctx* ctx, const prr_frame_info* info, const uint8_t* dev_packet, int idct,
+                     uint16_t* dev_samples, prr_dev_status* dev_status, uint32_t* dev_skipped,
+                     void* dev_scratch, size_t scratch_bytes);
+int prr_decode_reduced_async(prr_ctx* ctx, const prr_frame_info* info, const uint8_t* dev_packet,
+                             int scale, int greens, uint16_t* dev_rgb, prr_dev_status* dev_status,
+                             uint32_t* dev_skipped, void* dev_scratch, size_t scratch_bytes);
+
+/* --- linearize ---------------------------------------------------------------- */
+/* Frame::linearize_into, src/decoder.rs:197-216: coded code values (device)
+ * -> width*height linear values (device). Asynchronous. */
+int prr_linearize(prr_ctx* ctx, const prr_header* header, const uint16_t* dev_samples,
+                  uint16_t* dev_out, size_t out_len);
+
+/* --- develop ------------------------------------------------------------------ */
+/* DemosaicParams::new, src/demosaic.rs:80-82 */
+int prr_params_new(const prr_header* header, uint32_t quantizer, prr_params* out);
+/* DemosaicParams::with_white_balance, src/demosaic.rs:86-106 */
+int prr_params_with_white_balance(const prr_header* header, uint32_t quantizer, float red,
+                                  float blue, prr_params* out);
+/* output_matrix, src/demosaic.rs:138-153 */
+int prr_output_matrix(const prr_header* header, int exposure, float m[9]);
+/* develop_into / develop_planar_into, src/demosaic.rs:223-261, on device
+ * buffers. Interleaved: `r` holds 3*w*h floats (g, b unused). Planar: r, g,
+ * b hold w*h floats each. Asynchronous. */
+int prr_develop(prr_ctx* ctx, const prr_header* header, const prr_params* params, int stage,
+                const uint16_t* dev_samples, int layout, float* r, float* g, float* b,
+                size_t out_len);
+
+/* --- host-buffer conveniences (synchronous) ----------------------------------- */
+/* decode_frame_with + develop_planar_into / develop_into with host input and
+ * host outputs: uploads the packet, decodes and develops on the device and
+ * copies the result back. params NULL: DemosaicParams::new(header,
+ * Frame::quantizer). */
+int prr_decode_develop_host(prr_ctx* ctx, const uint8_t* packet, size_t len, int idct,
+                            const prr_params* params, int stage, int layout, float* r, float* g,
+                            float* b, size_t out_len, prr_decode_result* res, prr_error* err);
+
+/* --- diagnostics -------------------------------------------------------------- */
+/* The device inverse transforms on raw blocks (idct.rs): kind 0 Apple 8x8,
+ * 1 FFmpeg 8x8, 2 Apple 4x4 (16 coefficients per block), 3 Apple 2x2 (4).
+ * q always holds 64 entries per block. Device buffers; asynchronous. */
+int prr_transform_blocks(prr_ctx* ctx, int kind, const int16_t* dev_coefs, const int16_t* dev_q,
+                         uint16_t* dev_out, size_t nblocks);
+/* decode_component_reduced (src/coefficients.rs:203-312) on the device for
+ * n streams of one packet: stream i at byte dev offset off[i] (alignment =
+ * off[i] & 3) of length len[i], writing (64 or 16 or 4) << log2_blocks
+ * coefficients per stream (not dequantized). off/len are device arrays. */
+int prr_decode_components(prr_ctx* ctx, const uint8_t* dev_packet, const uint32_t* dev_off,
+                          const uint32_t* dev_len, size_t n, int log2_blocks, int log2_coefs,
+                          int16_t* dev_coefs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
