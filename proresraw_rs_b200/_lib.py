@@ -1,0 +1,173 @@
+"""ctypes declarations of include/prr.h (libprr.so)."""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libprr.so")
+HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "prr.h")
+
+OK = 0
+ERR_TRUNCATED = -1
+ERR_FRAME_SIZE_MISMATCH = -2
+ERR_BAD_QUANT_MATRIX = -3
+ERR_BAD_CURVE = -4
+ERR_UNEXPECTED_CURVE = -5
+ERR_BAD_TAG = -6
+ERR_HEADER_TOO_SHORT = -7
+ERR_UNSUPPORTED_VERSION = -8
+ERR_BAD_DIMENSIONS = -9
+ERR_BAD_ALIGNMENT = -10
+ERR_TILE_OUT_OF_BOUNDS = -11
+ERR_BAD_TILE_HEADER = -12
+ERR_BUFFER = -20
+ERR_CUDA = -21
+ERR_TIMEOUT = -22
+ERR_INVALID = -23
+ERR_NO_MEMORY = -24
+
+
+class CError(C.Structure):
+    _fields_ = [
+        ("code", C.c_int32),
+        ("what", C.c_char * 32),
+        ("needed", C.c_uint64),
+        ("available", C.c_uint64),
+        ("declared", C.c_uint32),
+        ("actual", C.c_uint64),
+        ("index", C.c_uint64),
+        ("value", C.c_uint32),
+        ("width", C.c_uint16),
+        ("height", C.c_uint16),
+        ("curve", C.c_uint16 * 8),
+        ("tag", C.c_uint8 * 4),
+    ]
+
+
+class CHeader(C.Structure):
+    _fields_ = [
+        ("version", C.c_uint8),
+        ("vendor", C.c_uint8 * 4),
+        ("bayer_pattern", C.c_uint8),
+        ("width", C.c_uint16),
+        ("height", C.c_uint16),
+        ("crop", C.c_uint8 * 4),
+        ("white_level", C.c_uint16),
+        ("wb_cct", C.c_uint16),
+        ("flags", C.c_uint16),
+        ("alignment", C.c_uint8),
+        ("pad0", C.c_uint8),
+        ("wb_red", C.c_float),
+        ("wb_blue", C.c_float),
+        ("color_matrix", C.c_float * 9),
+        ("gain", C.c_float),
+        ("quant_matrix", C.c_uint8 * 64),
+        ("curve", C.c_uint16 * 8),
+    ]
+
+
+class CFrameInfo(C.Structure):
+    _fields_ = [
+        ("header", CHeader),
+        ("packet_len", C.c_uint64),
+        ("table_offset", C.c_uint64),
+        ("ntiles", C.c_uint32),
+        ("tiles_per_row", C.c_uint32),
+        ("tile_rows", C.c_uint32),
+        ("coded_width", C.c_uint32),
+        ("coded_height", C.c_uint32),
+        ("pad0", C.c_uint32),
+    ]
+
+
+class CParams(C.Structure):
+    _fields_ = [
+        ("cfa_phase", C.c_int32),
+        ("black", C.c_int32),
+        ("one_over_range", C.c_float),
+        ("noise", C.c_float * 3),
+        ("clip", C.c_float * 2),
+        ("black_over_range", C.c_float),
+        ("wb", C.c_float * 2),
+    ]
+
+
+class CDecodeResult(C.Structure):
+    _fields_ = [
+        ("header", CHeader),
+        ("n_skipped", C.c_uint64),
+        ("skipped", C.POINTER(C.c_uint64)),
+        ("skipped_cap", C.c_uint64),
+        ("max_qscale", C.c_uint8),
+        ("pad", C.c_uint8 * 7),
+    ]
+
+
+class CDevStatus(C.Structure):
+    _fields_ = [
+        ("oob_tile", C.c_uint32),
+        ("n_skipped", C.c_uint32),
+        ("max_qscale", C.c_uint32),
+        ("error", C.c_uint32),
+    ]
+
+
+_lib = None
+
+
+def exported_names():
+    """Function names declared in include/prr.h."""
+    src = open(HEADER_PATH).read()
+    return sorted(set(re.findall(r"^\s*(?:[\w\s\*]+?)\b(prr_\w+)\s*\(", src, re.M)))
+
+
+def lib():
+    """Load libprr.so; raise if it is missing (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is missing: the CUDA library must be built "
+            "(python -m proresraw_rs_b200.build); there is no CPU fallback"
+        )
+    L = C.CDLL(LIB_PATH)
+    vp, sz, i = C.c_void_p, C.c_size_t, C.c_int
+    P = C.POINTER
+    sig = {
+        "prr_ctx_create": (i, [i, vp, P(vp)]),
+        "prr_ctx_destroy": (None, [vp]),
+        "prr_ctx_stream": (vp, [vp]),
+        "prr_sync": (i, [vp]),
+        "prr_status_string": (C.c_char_p, [i]),
+        "prr_last_error_string": (C.c_char_p, [vp]),
+        "prr_padded_packet_bytes": (sz, [sz]),
+        "prr_kernel_launches": (C.c_uint64, []),
+        "prr_header_len": (i, [vp, sz, P(sz), P(CError)]),
+        "prr_parse_header": (i, [vp, sz, P(CHeader), P(CError)]),
+        "prr_frame_info_parse": (i, [vp, sz, P(CFrameInfo), P(CError)]),
+        "prr_parse_frame": (i, [vp, sz, P(CFrameInfo), P(C.c_uint8), P(CError)]),
+        "prr_decode": (i, [vp, vp, sz, i, vp, sz, P(CDecodeResult), P(CError)]),
+        "prr_decode_reduced": (i, [vp, vp, sz, i, i, vp, sz, P(CDecodeResult), P(CError)]),
+        "prr_decode_scratch_bytes": (sz, [P(CFrameInfo)]),
+        "prr_decode_async": (i, [vp, P(CFrameInfo), vp, i, vp, vp, vp, vp, sz]),
+        "prr_decode_reduced_async": (i, [vp, P(CFrameInfo), vp, i, i, vp, vp, vp, vp, sz]),
+        "prr_linearize": (i, [vp, P(CHeader), vp, vp, sz]),
+        "prr_params_new": (i, [P(CHeader), C.c_uint32, P(CParams)]),
+        "prr_params_with_white_balance": (i, [P(CHeader), C.c_uint32, C.c_float, C.c_float, P(CParams)]),
+        "prr_output_matrix": (i, [P(CHeader), i, vp]),
+        "prr_develop": (i, [vp, P(CHeader), P(CParams), i, vp, i, vp, vp, vp, sz]),
+        "prr_decode_develop_host": (i, [vp, vp, sz, i, P(CParams), i, i, vp, vp, vp, sz, P(CDecodeResult),
+                                        P(CError)]),
+        "prr_transform_blocks": (i, [vp, i, vp, vp, vp, sz]),
+        "prr_decode_components": (i, [vp, vp, vp, vp, sz, i, i, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L

@@ -1,0 +1,358 @@
+// develop.cu -- linearization and the raw conversion (demosaic, white
+// balance, output matrix) on sm_100a.
+//
+// k_develop fuses the crate's three passes (src/demosaic.rs:356-398) into one
+// kernel over 32x32 output tiles:
+//  1. normalized values (curve folded with (v - black) / range,
+//     src/demosaic.rs:293-298) of the tile plus a 3-sensel halo, loaded with
+//     the picture-edge clamping the passes use, into shared memory;
+//  2. the green pass (src/demosaic.rs:481-541) over the tile plus a 1-sensel
+//     halo, keeping in shared memory the (red or blue, green) pair of every
+//     sensel and the per-sensel noise terms the chroma pass needs (variance
+//     and its square root), each computed once instead of once per use;
+//  3. the chroma pass (src/demosaic.rs:572-688) and the matrix
+//     (src/demosaic.rs:700-720) per 2x2 Bayer quad, so a thread's work does
+//     not depend on its column parity, with 8-byte coalesced stores.
+// Every operation is an IEEE round-to-nearest intrinsic, with fused
+// multiply-adds exactly where the crate calls mul_add, so the output is bit
+// for bit the crate's.
+
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace prr {
+
+namespace {
+
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float dv(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float rt(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+struct Noise {
+    float a, b, c;
+};
+
+// variance, src/demosaic.rs:423-426.
+__device__ __forceinline__ float variance(float v, float off, const Noise& n) {
+    const float t = add(off, v);
+    return add(n.c, fmaxf(n.b, mul(n.a, mul(t, t))));
+}
+
+// dot4, src/demosaic.rs:431-433.
+__device__ __forceinline__ float dot4(float a0, float a1, float a2, float a3, float b0, float b1,
+                                      float b2, float b3) {
+    return fma_(a3, b3, fma_(a2, b2, fma_(a0, b0, mul(a1, b1))));
+}
+
+// mirror, src/demosaic.rs:547-557.
+__device__ __forceinline__ void mirror(float* d, int pos, int len, float c) {
+    if (pos == 0) {
+        d[0] = d[1];
+        d[2] = d[3];
+    } else if (pos == 1) {
+        d[2] = c;
+    } else if (pos == len - 1) {
+        d[1] = d[0];
+        d[3] = d[2];
+    } else if (pos == len - 2) {
+        d[3] = c;
+    }
+}
+
+// estimate, src/demosaic.rs:572-604, with the per-sensel terms precomputed:
+// var_x = variance(x), sx = sqrt(var_x), sg = sqrt(variance(g)).
+__device__ __forceinline__ float estimate(const float* xx, const float* gg, const float* var_x,
+                                          const float* sx, const float* sg, float cg, float cs) {
+    const float mean_x = dot4(xx[0], xx[1], xx[2], xx[3], 0.25f, 0.25f, 0.25f, 0.25f);
+    // Also falls back when the comparison is unordered (NaN).
+    if (!(cs < cg)) return mean_x;
+    bool above = true;
+#pragma unroll
+    for (int i = 0; i < 4; i++) above &= (sx[i] < xx[i]) & (sg[i] < gg[i]);
+    if (!above) return mean_x;
+    float lo[4], mid[4], hi[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        lo[i] = dv(mul(sub(cg, cs), sub(xx[i], sx[i])), add(sg[i], gg[i]));
+        mid[i] = dv(mul(cg, xx[i]), gg[i]);
+        hi[i] = dv(mul(add(cs, cg), add(sx[i], xx[i])), sub(gg[i], sg[i]));
+    }
+    const float spread = dot4(sub(mid[0], lo[0]), sub(mid[1], lo[1]), sub(mid[2], lo[2]), sub(mid[3], lo[3]),
+                              sub(hi[0], mid[0]), sub(hi[1], mid[1]), sub(hi[2], mid[2]), sub(hi[3], mid[3]));
+    const float mean_mid = dot4(mid[0], mid[1], mid[2], mid[3], 0.25f, 0.25f, 0.25f, 0.25f);
+    const float dm0 = sub(mid[0], mean_mid), dm1 = sub(mid[1], mean_mid), dm2 = sub(mid[2], mean_mid),
+                dm3 = sub(mid[3], mean_mid);
+    const float b = fma_(spread, 0.75f, dot4(dm0, dm1, dm2, dm3, dm0, dm1, dm2, dm3));
+    const float dx0 = sub(xx[0], mean_x), dx1 = sub(xx[1], mean_x), dx2 = sub(xx[2], mean_x),
+                dx3 = sub(xx[3], mean_x);
+    const float vsum = dot4(var_x[0], var_x[1], var_x[2], var_x[3], 1.0f, 1.0f, 1.0f, 1.0f);
+    const float a = fma_(vsum, 0.75f, dot4(dx0, dx1, dx2, dx3, dx0, dx1, dx2, dx3));
+    const float weight = dv(a, add(b, a));
+    return fma_(sub(mean_mid, mean_x), weight, mean_x);
+}
+
+constexpr int TW = 32, TH = 32;           // output tile
+constexpr int NW = TW + 6, NH = TH + 6;   // normalized values, 3-sensel halo
+constexpr int GW = TW + 2, GH = TH + 2;   // green-pass region, 1-sensel halo
+constexpr int kDevThreads = 256;          // one thread per 2x2 quad of the tile
+
+struct DevShared {
+    float nrm[NH][NW];
+    float rb[GH][GW];   // red or blue (0 at green sites)
+    float gr[GH][GW];   // green
+    float vx[GH][GW];   // variance(rb) with the chroma offset (red/blue sites)
+    float sx[GH][GW];   // sqrt(vx)
+    float sg[GH][GW];   // sqrt(variance(green)) with the chroma offset
+    uint32_t c0[8], cd[8];
+};
+
+}  // namespace
+
+__global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
+    __shared__ DevShared S;
+    const int tid = threadIdx.x;
+    const int w = d.w, h = d.h;
+    const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    if (tid < 8) {
+        S.c0[tid] = d.curve_c0[tid];
+        S.cd[tid] = d.curve_delta[tid];
+    }
+    __syncthreads();
+    // 1. Normalized values, coordinates clamped to the picture as the green
+    //    pass clamps them (src/demosaic.rs:370-375, 499).
+    for (int i = tid; i < NH * NW; i += kDevThreads) {
+        const int ty = i / NW, tx = i - ty * NW;
+        const int y = min(max(y0 - 3 + ty, 0), h - 1);
+        const int x = min(max(x0 - 3 + tx, 0), w - 1);
+        const uint32_t code = __ldg(d.codes + size_t(y) * d.stride + x);
+        const int32_t lin = int32_t(curve_apply(S.c0, S.cd, code));
+        S.nrm[ty][tx] = mul(d.one_over_range, __int2float_rn(lin - d.black));
+    }
+    __syncthreads();
+    const Noise nz{d.noise[0], d.noise[1], d.noise[2]};
+    const int red_row = d.cfa >> 1, red_col = d.cfa & 1;
+    // 2. Green pass on the region: red/blue sites first (the heavy ones),
+    //    17 per region row, then green sites.
+    for (int k = tid; k < GH * (GW / 2) * 2; k += kDevThreads) {
+        const bool rbsite = k < GH * (GW / 2);
+        const int kk = rbsite ? k : k - GH * (GW / 2);
+        const int gy = kk / (GW / 2), j = kk - gy * (GW / 2);
+        const int y = y0 - 1 + gy;
+        const bool phase = (y & 1) == red_row;
+        const int first = phase ? red_col : 1 - red_col;
+        // Region column gx maps to x = x0 - 1 + gx with x0 even.
+        const int gx = 2 * j + (rbsite ? 1 - first : first);
+        const int x = x0 - 1 + gx;
+        if (y < 0 || y >= h || x < 0 || x >= w) continue;
+        const int ty = gy + 2, tx = gx + 2;  // nrm coordinates
+        const float centre = S.nrm[ty][tx];
+        float rbv = 0.0f, gv_out = centre;
+        if (rbsite) {
+            const float clip = phase ? d.clip[0] : d.clip[1];
+            const float c = fminf(centre, clip);
+            const float bs = d.green_off;
+            float hh[4] = {fminf(S.nrm[ty][tx - 1], 1.0f), fminf(S.nrm[ty][tx + 1], 1.0f),
+                           fminf(S.nrm[ty][tx - 2], clip), fminf(S.nrm[ty][tx + 2], clip)};
+            float vv[4] = {fminf(S.nrm[ty - 1][tx], 1.0f), fminf(S.nrm[ty + 1][tx], 1.0f),
+                           fminf(S.nrm[ty - 2][tx], clip), fminf(S.nrm[ty + 2][tx], clip)};
+            mirror(hh, x, w, c);
+            mirror(vv, y, h, c);
+            float var_h[4], var_v[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                var_h[i] = variance(hh[i], bs, nz);
+                var_v[i] = variance(vv[i], bs, nz);
+            }
+            const float sums0 = add(hh[0], hh[1]), sums1 = add(vv[0], vv[1]);
+            const float sums2 = add(hh[2], hh[3]), sums3 = add(vv[2], vv[3]);
+            float ratio0 = 0.0f, ratio1 = 0.0f;
+            if (c > rt(variance(c, bs, nz))) {
+                const float t0 = add(mul(c, 2.0f), sums2), t1 = add(mul(c, 2.0f), sums3);
+                const float t2 = add(mul(c, -2.0f), sums2), t3 = add(mul(c, -2.0f), sums3);
+#pragma unroll
+                for (int dir = 0; dir < 2; dir++) {
+                    const float* dd = dir == 0 ? hh : vv;
+                    const float* vd = dir == 0 ? var_h : var_v;
+                    float sd[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) sd[i] = rt(vd[i]);
+                    const float a = sub(dd[0], dd[1]);
+                    const float b = sub(dd[2], dd[3]);
+                    const bool any = mul(a, b) > 0.0f || mul(sub(dd[2], c), sub(dd[3], c)) > 0.0f ||
+                                     add(sd[0], sd[1]) > fabsf(a) || add(sd[2], sd[3]) > fabsf(b);
+                    const bool all = dd[0] > sd[0] && dd[1] > sd[1] && dd[2] > sd[2] && dd[3] > sd[3];
+                    if (any && all) {
+                        if (dir == 0)
+                            ratio0 = dv(t2, mul(t0, 2.0f));
+                        else
+                            ratio1 = dv(t3, mul(t1, 2.0f));
+                    }
+                }
+            }
+            const float gh = mul(mul(sums0, 0.5f), sub(1.0f, ratio0));
+            const float gvv = mul(mul(sums1, 0.5f), sub(1.0f, ratio1));
+            const float dh0 = sub(hh[0], gh), dh1 = sub(hh[1], gh), dh2 = sub(hh[2], c), dh3 = sub(hh[3], c);
+            const float dv0 = sub(vv[0], gvv), dv1 = sub(vv[1], gvv), dv2 = sub(vv[2], c), dv3 = sub(vv[3], c);
+            const float eh = add(dot4(dh0, dh1, dh2, dh3, dh0, dh1, dh2, dh3), add(var_h[0], var_h[1]));
+            const float ev = add(dot4(dv0, dv1, dv2, dv3, dv0, dv1, dv2, dv3), add(var_v[0], var_v[1]));
+            rbv = c;
+            gv_out = add(gvv, dv(mul(sub(gh, gvv), ev), add(eh, ev)));
+            const float vxx = variance(rbv, d.chroma_off, nz);
+            S.vx[gy][gx] = vxx;
+            S.sx[gy][gx] = rt(vxx);
+        }
+        S.rb[gy][gx] = rbv;
+        S.gr[gy][gx] = gv_out;
+        S.sg[gy][gx] = rt(variance(gv_out, d.chroma_off, nz));
+    }
+    __syncthreads();
+    // 3. Chroma (+ matrix) per quad.
+    const int qx = tid & 15, qy = tid >> 4;
+    const int xb = x0 + 2 * qx, yb = y0 + 2 * qy;
+    if (xb >= w || yb >= h) return;
+    float out[2][2][3];
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++) {
+        const int y = yb + dy;
+        const int ym = y > 0 ? y - 1 : y + 1, yp = y < h - 1 ? y + 1 : y - 1;
+        const int gy = y - y0 + 1, gym = ym - y0 + 1, gyp = yp - y0 + 1;
+        const bool on_red_row = (y & 1) == red_row;
+        const int rb_col = on_red_row ? red_col : 1 - red_col;
+#pragma unroll
+        for (int dx = 0; dx < 2; dx++) {
+            const int x = xb + dx;
+            const int xm = x > 0 ? x - 1 : x + 1, xp = x < w - 1 ? x + 1 : x - 1;
+            const int gx = x - x0 + 1, gxm = xm - x0 + 1, gxp = xp - x0 + 1;
+            const float c = S.rb[gy][gx], g = S.gr[gy][gx], cs = S.sg[gy][gx];
+            float r, b;
+            if ((x & 1) == rb_col) {
+                const int ny[4] = {gym, gyp, gym, gyp}, nx[4] = {gxm, gxm, gxp, gxp};
+                float xx[4], gg[4], vx[4], sx[4], sg[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    xx[i] = S.rb[ny[i]][nx[i]];
+                    gg[i] = S.gr[ny[i]][nx[i]];
+                    vx[i] = S.vx[ny[i]][nx[i]];
+                    sx[i] = S.sx[ny[i]][nx[i]];
+                    sg[i] = S.sg[ny[i]][nx[i]];
+                }
+                const float e = estimate(xx, gg, vx, sx, sg, g, cs);
+                r = on_red_row ? c : e;
+                b = on_red_row ? e : c;
+            } else {
+                // Each of two opposite neighbours counts twice.
+                auto pair = [&](int uy, int ux, int vy, int vx_) {
+                    const float xu = S.rb[uy][ux], xv = S.rb[vy][vx_];
+                    const float gu = S.gr[uy][ux], gv = S.gr[vy][vx_];
+                    const float vu = S.vx[uy][ux], vvv = S.vx[vy][vx_];
+                    const float su = S.sx[uy][ux], sv = S.sx[vy][vx_];
+                    const float tu = S.sg[uy][ux], tv = S.sg[vy][vx_];
+                    const float xx[4] = {xu, xv, xu, xv}, gg[4] = {gu, gv, gu, gv};
+                    const float vx4[4] = {vu, vvv, vu, vvv}, sx4[4] = {su, sv, su, sv};
+                    const float sg4[4] = {tu, tv, tu, tv};
+                    return estimate(xx, gg, vx4, sx4, sg4, g, cs);
+                };
+                const float eh = pair(gy, gxm, gy, gxp);
+                const float ev = pair(gym, gx, gyp, gx);
+                r = on_red_row ? eh : ev;
+                b = on_red_row ? ev : eh;
+            }
+            float rr = fminf(mul(r, d.wb[0]), 1.0f);
+            float gg = fminf(g, 1.0f);
+            float bb = fminf(mul(b, d.wb[1]), 1.0f);
+            if (d.has_matrix) {
+                const float m0 = fma_(bb, d.m[2], fma_(rr, d.m[0], mul(gg, d.m[1])));
+                const float m1 = fma_(bb, d.m[5], fma_(rr, d.m[3], mul(gg, d.m[4])));
+                const float m2 = fma_(bb, d.m[8], fma_(rr, d.m[6], mul(gg, d.m[7])));
+                rr = m0;
+                gg = m1;
+                bb = m2;
+            }
+            out[dy][dx][0] = rr;
+            out[dy][dx][1] = gg;
+            out[dy][dx][2] = bb;
+        }
+    }
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++) {
+        const size_t p = size_t(yb + dy) * w + xb;
+        if (d.layout == PRR_PLANAR) {
+            *reinterpret_cast<float2*>(d.r + p) = make_float2(out[dy][0][0], out[dy][1][0]);
+            *reinterpret_cast<float2*>(d.g + p) = make_float2(out[dy][0][1], out[dy][1][1]);
+            *reinterpret_cast<float2*>(d.b + p) = make_float2(out[dy][0][2], out[dy][1][2]);
+        } else {
+            float2* o = reinterpret_cast<float2*>(d.r + 3 * p);
+            o[0] = make_float2(out[dy][0][0], out[dy][0][1]);
+            o[1] = make_float2(out[dy][0][2], out[dy][1][0]);
+            o[2] = make_float2(out[dy][1][1], out[dy][1][2]);
+        }
+    }
+}
+
+// Frame::linearize_into (src/decoder.rs:197-216): eight sensels per thread.
+struct CurveDesc {
+    uint32_t c0[8], cd[8];
+};
+
+__global__ void k_linearize(const uint16_t* __restrict__ codes, uint32_t stride, int w, int h,
+                            CurveDesc curve, uint16_t* __restrict__ out, int vec_out) {
+    __shared__ uint32_t c0[8], cd[8];
+    if (threadIdx.x < 8) {
+        c0[threadIdx.x] = curve.c0[threadIdx.x];
+        cd[threadIdx.x] = curve.cd[threadIdx.x];
+    }
+    __syncthreads();
+    const int cpr = (w + 7) / 8;
+    const size_t idx = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int y = int(idx / cpr);
+    if (y >= h) return;
+    const int xc = int(idx - size_t(y) * cpr) * 8;
+    const uint16_t* src = codes + size_t(y) * stride + xc;
+    uint16_t* dst = out + size_t(y) * w + xc;
+    if (xc + 8 <= w) {
+        const uint4 raw = __ldg(reinterpret_cast<const uint4*>(src));
+        const uint16_t* in = reinterpret_cast<const uint16_t*>(&raw);
+        __align__(16) uint16_t v[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) v[k] = uint16_t(curve_apply(c0, cd, in[k]));
+        if (vec_out) {
+            *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(v);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) dst[k] = v[k];
+        }
+    } else {
+        for (int k = 0; xc + k < w; k++) dst[k] = uint16_t(curve_apply(c0, cd, src[k]));
+    }
+}
+
+cudaError_t launch_linearize(const uint16_t* codes, uint32_t stride, int w, int h, const uint32_t* c0,
+                             const uint32_t* delta, uint16_t* out, cudaStream_t s) {
+    const size_t chunks = size_t((w + 7) / 8) * h;
+    if (chunks == 0) return cudaSuccess;
+    const int vec_out = (w % 8 == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+    const unsigned blocks = unsigned((chunks + 255) / 256);
+    CurveDesc curve;
+    for (int i = 0; i < 8; i++) {
+        curve.c0[i] = c0[i];
+        curve.cd[i] = delta[i];
+    }
+    k_linearize<<<blocks, 256, 0, s>>>(codes, stride, w, h, curve, out, vec_out);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_develop(const DevelopDesc& d, cudaStream_t s) {
+    if (d.w <= 0 || d.h <= 0) return cudaSuccess;
+    dim3 grid((d.w + TW - 1) / TW, (d.h + TH - 1) / TH);
+    k_develop<<<grid, kDevThreads, 0, s>>>(d);
+    count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace prr

@@ -1,0 +1,58 @@
+"""The C-ABI libraries load and export what their headers declare (no GPU
+needed: only loading and host-side entry points are exercised)."""
+
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import proresraw_rs_b200 as P
+from proresraw_rs_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared(header):
+    src = open(os.path.join(ROOT, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b((?:prr|prs)_\w+)\s*\(", src)))
+
+
+def test_libprr_exports_every_declared_symbol():
+    names = declared("prr.h")
+    assert len(names) >= 25
+    lib = C.CDLL(_lib.LIB_PATH)
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert missing == []
+
+
+def test_libprr_synth_exports_every_declared_symbol():
+    names = declared("prr_synth.h")
+    lib = C.CDLL(os.path.join(ROOT, "proresraw_rs_b200", "lib", "libprr_synth.so"))
+    assert [n for n in names if not hasattr(lib, n)] == []
+
+
+def test_status_strings_and_padding():
+    L = _lib.lib()
+    assert L.prr_status_string(0) == b"ok"
+    assert L.prr_status_string(-11) == b"tile out of bounds"
+    assert L.prr_padded_packet_bytes(1) >= 17
+    assert L.prr_padded_packet_bytes(100) % 16 == 0
+
+
+def test_scratch_size_covers_the_tile_offsets():
+    from proresraw_rs_b200 import synth as S
+
+    pkt = S.frame(S.Spec(5760, 64, alignment=4), [S.tile(1, [b"\x80"] * 4)] * S.ntiles(5760, 64, 4))
+    info = P.frame_info(pkt)
+    assert _lib.lib().prr_decode_scratch_bytes(C.byref(info)) >= 4 * (info.ntiles + 1)
+
+
+def test_the_library_refuses_to_run_without_a_device():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(RuntimeError):
+        P.context()
