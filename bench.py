@@ -289,8 +289,54 @@ def run(args):
     ms_max = float(t.item())
     value = world * args.steps / (ms_max / 1000.0)
 
-    # e2e: the host-buffer C-ABI call, pinned host packet in and planes out,
-    # with two contexts on two host threads so that copies overlap kernels.
+    e2e_value = None
+    if not args.no_e2e:
+        e2e_value = measure_e2e(args, L, _lib, pkts, n, world)
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        alg_bytes = 2 * n + 12 * n
+        achieved = alg_bytes / (dev_ms / 1000.0) / 1e9
+        traffic = traffic_from_profiles()
+        line = {
+            "metric": "5.8K frames/s decode+develop (bit-exact)",
+            "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16+f32", "data": "synthetic",
+            "config": {"workload": "5760x3040 BGGR v0 align4 qscale45 qmat[4,63] 0.5% corrupt tiles; "
+                                   "decode_frame(Apple) + develop_planar_into(Rec2020)",
+                       "frames_in_ring": RING, "packet_bytes": [len(p) for p in pkts],
+                       "l2": "inputs+outputs > L2 (210 MB planes written per step)",
+                       "parallelism": f"replicas x{world}",
+                       "decode_ms": dec_ms, "develop_ms": dev_ms},
+            "roofline": {"bound": "hbm", "kernel": "k_develop", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs",
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "gpu_launches": int(launches),
+        }
+        if e2e_value is not None:
+            line["e2e"] = {"value": e2e_value, "unit": "frames/s",
+                           "h2d_bytes_per_step": int(np.mean([len(p) for p in pkts])),
+                           "d2h_bytes_per_step": 12 * n + 16,
+                           "note": "prr_decode_develop_host from pinned host memory, 2 host threads, wall clock"}
+        cl = clocks.summary()
+        if cl:
+            line["clocks"] = cl
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(pkts)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def measure_e2e(args, L, _lib, pkts, n, world):
+    """Frames/s through prr_decode_develop_host: pinned host packet in,
+    pinned host planes out, with two contexts on two host threads so that
+    copies overlap kernels. Wall clock, max over ranks."""
+    import torch
+
     host_pkts = []
     for p in pkts:
         hp = torch.empty(len(p), dtype=torch.uint8, pin_memory=True)
@@ -338,41 +384,7 @@ def run(args):
     e2e_value = world * args.steps / float(te.item())
     for cx in ctxs:
         L.prr_ctx_destroy(cx)
-
-    if rank == 0:
-        peak, peak_kind = peaks()
-        alg_bytes = 2 * n + 12 * n
-        achieved = alg_bytes / (dev_ms / 1000.0) / 1e9
-        traffic = traffic_from_profiles()
-        line = {
-            "metric": "5.8K frames/s decode+develop (bit-exact)",
-            "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u16+f32", "data": "synthetic",
-            "config": {"workload": "5760x3040 BGGR v0 align4 qscale45 qmat[4,63] 0.5% corrupt tiles; "
-                                   "decode_frame(Apple) + develop_planar_into(Rec2020)",
-                       "frames_in_ring": RING, "packet_bytes": [len(p) for p in pkts],
-                       "l2": "inputs+outputs > L2 (210 MB planes written per step)",
-                       "parallelism": f"replicas x{world}",
-                       "decode_ms": dec_ms, "develop_ms": dev_ms},
-            "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": int(np.mean([len(p) for p in pkts])),
-                    "d2h_bytes_per_step": 12 * n + 16,
-                    "note": "prr_decode_develop_host from pinned host memory, 2 host threads, wall clock"},
-            "roofline": {"bound": "hbm", "kernel": "k_develop", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": f"{peak_kind} hbm_gbs",
-                         "algorithmic_bytes_per_launch": alg_bytes},
-            "gpu_launches": int(launches),
-        }
-        cl = clocks.summary()
-        if cl:
-            line["clocks"] = cl
-        if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(pkts)
-        print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.destroy_process_group()
-    return 0
+    return e2e_value
 
 
 def main():
@@ -382,6 +394,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

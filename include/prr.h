@@ -136,7 +136,9 @@ enum prr_layout { PRR_INTERLEAVED = 0, PRR_PLANAR = 1 };
 typedef struct prr_ctx prr_ctx;
 
 /* --- context ------------------------------------------------------------------ */
-/* One device and one CUDA stream (NULL: the context creates its own). */
+/* One device and one CUDA stream (NULL: the context creates its own
+ * non-blocking stream; pass cudaStreamLegacy, (void*)0x1, to run on the
+ * legacy default stream). */
 int prr_ctx_create(int device, void* cuda_stream, prr_ctx** out);
 void prr_ctx_destroy(prr_ctx* ctx);
 /* The stream the context enqueues on (a cudaStream_t). */

@@ -288,6 +288,7 @@ def frame_quantizer(parsed: ParsedFrame) -> int:
 # Contexts: one per (device, torch stream), so that the kernels run in
 # stream order with the torch tensors they read and write.
 
+_CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy in cuda_runtime_api.h
 _ctx_lock = threading.Lock()
 _contexts: Dict[Tuple[int, int], C.c_void_p] = {}
 
@@ -304,12 +305,16 @@ def context(device: Optional[int] = None) -> C.c_void_p:
         raise RuntimeError("proresraw_rs_b200 needs a CUDA device (there is no CPU path)")
     dev = torch.cuda.current_device() if device is None else device
     stream = torch.cuda.current_stream(dev).cuda_stream
+    # torch's default stream is the legacy NULL stream; a NULL handle would
+    # make the library create a stream of its own, so name the legacy
+    # stream explicitly (cudaStreamLegacy).
+    handle = stream if stream else _CUDA_STREAM_LEGACY
     key = (dev, stream)
     with _ctx_lock:
         ctx = _contexts.get(key)
         if ctx is None:
             ctx = C.c_void_p()
-            rc = _lib.lib().prr_ctx_create(dev, C.c_void_p(stream), C.byref(ctx))
+            rc = _lib.lib().prr_ctx_create(dev, C.c_void_p(handle), C.byref(ctx))
             if rc:
                 raise _error(rc)
             _contexts[key] = ctx
