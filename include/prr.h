@@ -50,7 +50,12 @@ enum prr_status {
     PRR_ERR_TIMEOUT = -22, /* a bounded device loop gave up; the context stays usable */
     PRR_ERR_INVALID = -23, /* an argument is out of range */
     PRR_ERR_NO_MEMORY = -24,
+    PRR_ERR_SCRATCH_LIMIT = -25, /* the frame has more tiles than prr_decode_noalloc's fixed scratch holds */
 };
+
+/* Largest tile count prr_decode_noalloc accepts (8192x4320 at alignment 0
+ * has 138,240 tiles). */
+#define PRR_NOALLOC_MAX_TILES 262144u
 
 /* Payload of an error: the fields of the matching `Error` variant. */
 typedef struct prr_error {
@@ -192,6 +197,26 @@ int prr_decode_async(prr_ctx* ctx, const prr_frame_info* info, const uint8_t* de
 int prr_decode_reduced_async(prr_ctx* ctx, const prr_frame_info* info, const uint8_t* dev_packet,
                              int scale, int greens, uint16_t* dev_rgb, prr_dev_status* dev_status,
                              uint32_t* dev_skipped, void* dev_scratch, size_t scratch_bytes);
+
+/* A full-resolution decode that allocates no memory at all, for callers
+ * that may not allocate device memory while they decode: plug-ins whose
+ * host application owns the device memory and passes in only the input and
+ * output buffers, and real-time loops in which a cudaMalloc would stall the
+ * device or could fail because another allocator has reserved it. No
+ * counterpart in the reference crate.
+ * The caller passes the packet (device, padded as for prr_decode_async),
+ * the code-value output, the status and the skipped-tile list; the one
+ * piece of scratch, the tile-offset table, is a fixed array of
+ * PRR_NOALLOC_MAX_TILES + 1 words inside the library, held by every device
+ * that loads the library until the process exits. Frames with more tiles
+ * return PRR_ERR_SCRATCH_LIMIT. The first call on a device looks the array
+ * up (with `device` made current) and should come before any stream
+ * capture on that device. All calls share the array: calls whose work
+ * overlaps on the GPU (other streams, other threads) race; serialize them
+ * on one stream. `cuda_stream` is a cudaStream_t (NULL: legacy default). */
+int prr_decode_noalloc(int device, void* cuda_stream, const prr_frame_info* info,
+                       const uint8_t* dev_packet, int idct, uint16_t* dev_samples,
+                       prr_dev_status* dev_status, uint32_t* dev_skipped);
 
 /* --- linearize ---------------------------------------------------------------- */
 /* Frame::linearize_into, src/decoder.rs:197-216: coded code values (device)

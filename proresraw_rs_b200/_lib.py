@@ -28,6 +28,8 @@ ERR_CUDA = -21
 ERR_TIMEOUT = -22
 ERR_INVALID = -23
 ERR_NO_MEMORY = -24
+ERR_SCRATCH_LIMIT = -25
+NOALLOC_MAX_TILES = 262144
 
 
 class CError(C.Structure):
@@ -164,6 +166,7 @@ def lib():
                                         P(CError)]),
         "prr_transform_blocks": (i, [vp, i, vp, vp, vp, sz]),
         "prr_decode_components": (i, [vp, vp, vp, vp, sz, i, i, vp]),
+        "prr_decode_noalloc": (i, [i, vp, P(CFrameInfo), vp, i, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

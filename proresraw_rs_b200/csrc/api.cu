@@ -247,6 +247,7 @@ const char* prr_status_string(int s) {
         case PRR_ERR_TIMEOUT: return "device loop bound reached";
         case PRR_ERR_INVALID: return "invalid argument";
         case PRR_ERR_NO_MEMORY: return "out of memory";
+        case PRR_ERR_SCRATCH_LIMIT: return "frame exceeds the fixed scratch of the no-alloc decode";
         default: return "unknown status";
     }
 }
