@@ -202,7 +202,7 @@ struct prr_ctx {
     bool own_stream = false;
     DevBuf<uint8_t> pkt;
     HostBuf<uint8_t> hpkt;
-    DevBuf<uint32_t> tile_off;
+    DevBuf<uint8_t> scratch;  // decode scratch (tile offsets, stream counts, coefficient lists)
     DevBuf<uint32_t> skipped;
     DevBuf<prr_dev_status> status;
     HostBuf<prr_dev_status> hstatus;
@@ -285,7 +285,7 @@ void prr_ctx_destroy(prr_ctx* c) {
     cudaStreamSynchronize(c->stream);
     c->pkt.release();
     c->hpkt.release();
-    c->tile_off.release();
+    c->scratch.release();
     c->skipped.release();
     c->status.release();
     c->hstatus.release();
@@ -391,7 +391,7 @@ int prr_parse_frame(const uint8_t* pkt, size_t len, prr_frame_info* out, uint8_t
 }
 
 size_t prr_decode_scratch_bytes(const prr_frame_info* info) {
-    return info ? ((size_t(info->ntiles) + 1) * 4 + 255) & ~size_t(255) : 0;
+    return info ? decode_scratch_layout(info->ntiles, info->coded_width, info->coded_height).total : 0;
 }
 
 }  // extern "C"
@@ -446,6 +446,21 @@ int finish_decode(prr_ctx* c, const prr_frame_info& f, prr_decode_result* res, p
     return PRR_OK;
 }
 
+// Enqueue a frame decode: the tile-offset scan, the entropy kernel and the
+// transform kernel, with the scratch laid out by decode_scratch_layout.
+int launch_frame(prr_ctx* c, const prr_frame_info& f, const uint8_t* dev_pkt, bool reduced, int idct,
+                 int scale, int greens, uint16_t* dev_out, prr_dev_status* st, uint32_t* skipped,
+                 uint8_t* scratch) {
+    const DecodeScratch l = decode_scratch_layout(f.ntiles, f.coded_width, f.coded_height);
+    FrameDesc d = make_frame_desc(f, dev_pkt);
+    uint32_t* tile_off = reinterpret_cast<uint32_t*>(scratch + l.tile_off);
+    d.counts = reinterpret_cast<uint32_t*>(scratch + l.counts);
+    d.pairs = reinterpret_cast<uint32_t*>(scratch + l.pairs);
+    PRR_TRY(c->cuda(launch_tile_index(d, tile_off, st, c->stream)));
+    if (reduced) return c->cuda(launch_decode_reduced(d, scale, greens, tile_off, st, skipped, dev_out, c->stream));
+    return c->cuda(launch_decode_full(d, idct, tile_off, st, skipped, dev_out, c->stream));
+}
+
 int decode_common(prr_ctx* c, const uint8_t* packet, size_t len, bool reduced, int idct, int scale,
                   int greens, uint16_t* dev_out, size_t out_len, prr_decode_result* res,
                   prr_error* err) {
@@ -463,16 +478,11 @@ int decode_common(prr_ctx* c, const uint8_t* packet, size_t len, bool reduced, i
     }
     const uint8_t* dev_pkt = nullptr;
     PRR_TRY(upload_packet(c, packet, len, &dev_pkt));
-    PRR_TRY(c->cuda(c->tile_off.ensure(size_t(f.ntiles) + 1)));
+    const size_t scratch_bytes = prr_decode_scratch_bytes(&f);
+    PRR_TRY(c->cuda(c->scratch.ensure(scratch_bytes)));
     PRR_TRY(c->cuda(c->skipped.ensure(f.ntiles)));
-    const FrameDesc d = make_frame_desc(f, dev_pkt);
-    PRR_TRY(c->cuda(launch_tile_index(d, c->tile_off.p, c->status.p, c->stream)));
-    if (reduced)
-        PRR_TRY(c->cuda(launch_decode_reduced(d, scale, greens, c->tile_off.p, c->status.p, c->skipped.p,
-                                              dev_out, c->stream)));
-    else
-        PRR_TRY(c->cuda(launch_decode_full(d, idct, c->tile_off.p, c->status.p, c->skipped.p, dev_out,
-                                           c->stream)));
+    PRR_TRY(launch_frame(c, f, dev_pkt, reduced, idct, scale, greens, dev_out, c->status.p, c->skipped.p,
+                         c->scratch.p));
     return finish_decode(c, f, res, err);
 }
 
@@ -485,12 +495,8 @@ int decode_async_common(prr_ctx* c, const prr_frame_info* info, const uint8_t* d
     if (reduced && (scale < 1 || scale > 3 || greens < 0 || greens > 1)) return PRR_ERR_INVALID;
     if (!reduced && idct != PRR_IDCT_APPLE && idct != PRR_IDCT_FFMPEG) return PRR_ERR_INVALID;
     PRR_TRY(c->use_device());
-    const FrameDesc d = make_frame_desc(*info, dev_packet);
-    uint32_t* tile_off = static_cast<uint32_t*>(scratch);
-    PRR_TRY(c->cuda(launch_tile_index(d, tile_off, st, c->stream)));
-    if (reduced)
-        return c->cuda(launch_decode_reduced(d, scale, greens, tile_off, st, skipped, dev_out, c->stream));
-    return c->cuda(launch_decode_full(d, idct, tile_off, st, skipped, dev_out, c->stream));
+    return launch_frame(c, *info, dev_packet, reduced, idct, scale, greens, dev_out, st, skipped,
+                        static_cast<uint8_t*>(scratch));
 }
 
 void params_wb(const prr_header* h, uint32_t quantizer, float red, float blue, prr_params* out) {

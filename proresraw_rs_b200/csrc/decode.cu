@@ -152,13 +152,22 @@ struct SegShared {
     uint8_t sq_valid[16];
     uint8_t qmat[64];
     uint32_t ntiles;
+    uint32_t first_j;  // index within the tile row of the segment's first tile
+    uint32_t sq0;      // first 16-sensel column of the segment
     __align__(16) int16_t coef[64 * kCoefStride];  // [square * 4 + stream][72]
     __align__(16) uint32_t rowbuf[64 * kRowStride];  // row-pass output, f32 or int32 bits
 };
 
-// Parse this segment's tiles and zero the coefficient buffer. `streams_mask`
-// selects the streams to be decoded; returns the number of 16-sensel columns
-// (squares) of the segment.
+// First entry of the (position, value) list of stream s of the tile whose
+// first square is column `sq_x` of tile row `trow`: the tile's squares own
+// 4 << log2_coefs entries each, so every tile's four lists are disjoint.
+__device__ __forceinline__ uint32_t stream_list_base(const FrameDesc& d, uint32_t trow, uint32_t sq_x,
+                                                     uint32_t log2, uint32_t s, uint32_t lc) {
+    return ((trow * d.columns + sq_x) * 4 + (s << log2)) << lc;
+}
+
+// Parse this segment's tiles and zero the coefficient buffer; returns the
+// number of 16-sensel columns (squares) of the segment.
 __device__ __forceinline__ uint32_t seg_setup(SegShared& S, const FrameDesc& d,
                                               const uint32_t* __restrict__ tile_off,
                                               prr_dev_status* st, uint32_t* skipped,
@@ -184,7 +193,11 @@ __device__ __forceinline__ uint32_t seg_setup(SegShared& S, const FrameDesc& d,
             here = x < sq0 + nsq;
         }
         const uint32_t count = __popc(__ballot_sync(0xFFFFFFFFu, here));
-        if (tid == 0) S.ntiles = count;
+        if (tid == 0) {
+            S.ntiles = count;
+            S.first_j = j0;
+            S.sq0 = sq0;
+        }
         if (here) {
             SegTile t;
             const uint32_t idx = trow * d.tiles_per_row + j;
@@ -244,11 +257,54 @@ __device__ __forceinline__ void seg_decode_stream(SegShared& S, const FrameDesc&
         const uint32_t qi = ((p >> hl) << 3) | (p & ((1u << hl) - 1));
         base[b * 4 * kCoefStride + p] = dequantize(v, int32_t(qm[qi]) * int32_t(qscale));
     };
-    if (!decode_component(d.words, t.soff[s], t.slen[s], t.log2, lc, S.T, store))
+    bool revisited = false;
+    if (!decode_component(GlobalWords{d.words}, t.soff[s], t.slen[s], t.log2, lc, S.T, store, revisited) && st)
         atomicOr(&st->error, 1u);
 }
 
-template <int IDCT>
+// Fill the segment's shared coefficients from the lists k_entropy wrote:
+// one warp per stream, lanes over the list's (position, value) entries.
+// A stream whose zero run wrapped back over stored positions may hold a
+// position twice; it is replayed in order by one lane so the later value
+// wins, as on the host.
+__device__ __forceinline__ void seg_scatter(SegShared& S, const FrameDesc& d, uint32_t trow,
+                                            uint32_t log2_coefs, bool second_green, prr_dev_status* st) {
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t lc = log2_coefs;
+    const uint32_t first_tile = trow * d.tiles_per_row + S.first_j;
+    for (uint32_t k = warp; k < 4 * S.ntiles; k += kThreads / 32) {
+        const uint32_t t = k >> 2, s = k & 3;
+        const SegTile& tl = S.tiles[t];
+        if (!tl.valid || (s == 1 && !second_green)) continue;
+        const uint32_t g = (first_tile + t) * 4 + s;
+        const uint32_t cnt = d.counts[g];
+        const uint32_t n = cnt & 0x7FFFFFFFu;
+        const uint32_t* list = d.pairs + stream_list_base(d, trow, tl.x_rel + S.sq0, tl.log2, s, lc);
+        int16_t* base = S.coef + (tl.x_rel * 4 + s) * kCoefStride;
+        // Entry: interleaved position n << 16 | raw 16-bit value. Placement
+        // (src/coefficients.rs:252-254) and dequantization (src/idct.rs:41-43)
+        // happen here, off the entropy decoder's serial chain.
+        const uint8_t* scan = lc == 6 ? S.T.scan : (lc == 4 ? S.T.scan4 : S.T.scan2);
+        const uint32_t hl = lc >> 1, mask = (1u << tl.log2) - 1;
+        const int32_t qscale = int32_t(tl.qscale);
+        auto put = [&](uint32_t e) {
+            const uint32_t nn = e >> 16;
+            const uint32_t p = scan[nn >> tl.log2];
+            const uint32_t qi = ((p >> hl) << 3) | (p & ((1u << hl) - 1));
+            base[(nn & mask) * 4 * kCoefStride + p] =
+                dequantize(int16_t(e & 0xFFFF), int32_t(S.qmat[qi]) * qscale);
+        };
+        if (cnt >> 31) {
+            // Positions revisited (and possibly more entries than the list
+            // holds): decode the stream again here, in order.
+            if (lane == 0) seg_decode_stream(S, d, t, s, lc, st);
+        } else {
+            for (uint32_t i = lane; i < n; i += 32) put(__ldg(list + i));
+        }
+    }
+}
+
+template <int IDCT, bool SPLIT>
 __global__ void __launch_bounds__(kThreads) k_decode_full(FrameDesc d, const uint32_t* __restrict__ tile_off,
                                                          prr_dev_status* __restrict__ st,
                                                          uint32_t* __restrict__ skipped,
@@ -257,8 +313,12 @@ __global__ void __launch_bounds__(kThreads) k_decode_full(FrameDesc d, const uin
     const uint32_t tid = threadIdx.x;
     const uint32_t seg = blockIdx.x, trow = blockIdx.y;
     const uint32_t nsq = seg_setup(S, d, tile_off, st, skipped, seg, trow);
-    // Entropy decoding: one thread per component stream.
-    if (tid < 4 * S.ntiles) seg_decode_stream(S, d, tid >> 2, tid & 3, 6, st);
+    if (SPLIT) {
+        seg_scatter(S, d, trow, 6, true, st);
+    } else {
+        // Entropy decoding in the CTA: one thread per component stream.
+        if (tid < 4 * S.ntiles) seg_decode_stream(S, d, tid >> 2, tid & 3, 6, st);
+    }
     __syncthreads();
     // Row pass: task = row * 64 + block; a warp shares one row (and its
     // table set), 32 blocks side by side.
@@ -336,7 +396,7 @@ __global__ void __launch_bounds__(kThreads) k_decode_full(FrameDesc d, const uin
 // Reduced-resolution decode (src/reduced.rs:217-273): red from stream 3,
 // green from stream 0 (averaged with stream 1 for Greens::Average), blue
 // from stream 2, through the 8x8, 4x4 or 2x2 transform and the curve.
-template <int SHIFT>
+template <int SHIFT, bool SPLIT>
 __global__ void __launch_bounds__(kThreads) k_decode_reduced(FrameDesc d, int greens,
                                                             const uint32_t* __restrict__ tile_off,
                                                             prr_dev_status* __restrict__ st,
@@ -353,7 +413,9 @@ __global__ void __launch_bounds__(kThreads) k_decode_reduced(FrameDesc d, int gr
         cd[tid] = d.curve_delta[tid];
     }
     const uint32_t nsq = seg_setup(S, d, tile_off, st, skipped, seg, trow);
-    {
+    if (SPLIT) {
+        seg_scatter(S, d, trow, LC, greens != 0, st);
+    } else {
         const uint32_t s = tid & 3;
         if (tid < 4 * S.ntiles && (s != 1 || greens)) seg_decode_stream(S, d, tid >> 2, s, LC, st);
     }
@@ -450,6 +512,167 @@ __global__ void __launch_bounds__(kThreads) k_decode_reduced(FrameDesc d, int gr
 }
 
 // ---------------------------------------------------------------------------
+// Entropy decoding apart from the transform: one thread per component
+// stream, streams in frame order (tile-major), so a warp decodes the 32
+// streams of 8 neighbouring tiles side by side. Each thread parses its tile's
+// header (Tile::parse, src/tile.rs:126-153) and appends every coefficient
+// its stream stores as an (interleaved position n << 16 | raw 16-bit value)
+// entry to its stream's list, four entries per 16-byte store; counts[g]
+// gets the entry count. Placement and dequantization are left to the
+// transform kernel so that the serial symbol chain stays short. A stream
+// whose zero run wrapped back over stored positions (malformed input only)
+// gets bit 31 instead and is decoded again, in order, by the transform
+// kernel; its list is never written past its capacity. Invalid tiles are
+// left to the transform kernel, which records them.
+//
+// The symbol loop is decode_component_reduced (src/coefficients.rs:203-312)
+// as a state machine, one symbol per iteration; the codebook lookups of all
+// states are issued together and the state's own update picks its result.
+template <uint32_t LC, class Src>
+__device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off, uint32_t len,
+                                                   uint32_t log2_blocks, const CodeTables& T, uint32_t* list,
+                                                   bool& revisited, bool& ok) {
+    const uint32_t blocks = 1u << log2_blocks;
+    const uint32_t codes = blocks << LC;
+    Reader<Src> r;
+    r.init(src, off, len);
+    uint32_t cnt = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+    // Append the coefficient at interleaved position n (DCs are 0..blocks-1).
+    auto append = [&](uint32_t n, uint32_t value) {
+        e0 = e1;
+        e1 = e2;
+        e2 = e3;
+        e3 = (n << 16) | (value & 0xFFFF);
+        if ((cnt & 3) == 3) *reinterpret_cast<uint4*>(list + cnt - 3) = make_uint4(e0, e1, e2, e3);
+        cnt++;
+    };
+    bool live = r.top() != 0;
+    // DC: the sign-folded first value, then deltas with a running sign
+    // (src/coefficients.rs:225-248).
+    if (live) {
+        uint32_t l;
+        const uint32_t v = codeword(r.top(), FIRST_DC, l);
+        r.consume(l);
+        const uint32_t odd = v & 1;
+        int32_t dc = int32_t((((odd + v) >> 1) ^ (0u - odd)) + odd);
+        append(0, uint32_t(dc));
+        uint32_t dc_cb = DC_RESET, sign = 0;
+        for (uint32_t block = 1; block < blocks; block++) {
+            if (r.top() == 0) {
+                live = false;
+                break;
+            }
+            const uint32_t s = codeword(r.top(), dc_cb, l);
+            sign ^= s & 1;
+            const uint32_t magnitude = ((s & 1) + s) >> 1;
+            const int32_t delta = int32_t(((0u - sign) ^ magnitude) + sign);
+            dc_cb = T.dc[min(magnitude, 12u)];
+            sign = delta < 0 ? 1u : 0u;
+            r.consume(l);
+            dc = int32_t(uint32_t(dc) + uint32_t(delta));
+            append(block, uint32_t(dc));
+        }
+    }
+    // AC (src/coefficients.rs:271-311) as four states, updated with selects
+    // so that lanes in different states run the same instructions: the
+    // length of a non-zero run, a level inside the run, a zero run, the level
+    // after a zero run.
+    enum : uint32_t { RUN_LENGTH = 0, ZEROS = 1, LEVELS = 2, LEVEL = 3 };
+    uint32_t state = RUN_LENGTH, cb = LN_INITIAL;
+    uint32_t ac_cb = AC_INITIAL, rn_cb = RN_INITIAL, ln_cb = LN_INITIAL;
+    uint32_t n = blocks, run = 0;
+    uint32_t budget = 64u * (8u * len + 64u) + 4u * codes;
+    while (live) {
+        const uint32_t top = r.top();
+        if (top == 0) break;  // end of component
+        if (budget-- == 0) {
+            ok = false;
+            break;
+        }
+        uint32_t l;
+        const uint32_t v = codeword(top, cb, l);
+        const bool is_level = state >= LEVELS;
+        const bool negative = int32_t(top << (l & 31)) < 0;
+        r.consume(l + (is_level ? 1u : 0u));
+        const uint32_t ac_next = T.ac[min(v, 94u)];
+        const uint32_t ln_next = T.ln[min(v, 14u)];
+        const uint32_t rn_next = T.rn[min(v, 27u)];
+        if (is_level) {
+            const uint32_t mag = (v + 1) & 0xFFFF;
+            if (cnt < codes) append(n, negative ? (0u - mag) : mag);
+        }
+        const bool rl = state == RUN_LENGTH, zr = state == ZEROS, l1 = state == LEVEL;
+        // A zero run is zeros + 1 long and wraps like the crate's u32.
+        const uint32_t n_new = zr ? n + 1 + v : n + (is_level ? 1u : 0u);
+        revisited |= zr && n_new < n;
+        n = n_new;
+        ac_cb = is_level ? ac_next : ac_cb;
+        ln_cb = l1 ? ln_next : ln_cb;
+        rn_cb = zr ? rn_next : rn_cb;
+        run = rl ? v : (state == LEVELS ? run - 1 : run);
+        if ((zr || is_level) && n >= codes) break;
+        state = rl ? (v > 0 ? LEVELS : ZEROS) : zr ? LEVEL : l1 ? RUN_LENGTH : (run == 0 ? ZEROS : LEVELS);
+        cb = state >= LEVELS ? ac_cb : (state == RUN_LENGTH ? ln_cb : rn_cb);
+    }
+    // Entries still in registers: the last cnt & 3 of e1..e3.
+    const uint32_t rem = cnt & 3;
+    if (rem >= 1) list[cnt - rem] = rem == 3 ? e1 : (rem == 2 ? e2 : e3);
+    if (rem >= 2) list[cnt - rem + 1] = rem == 3 ? e2 : e3;
+    if (rem >= 3) list[cnt - rem + 2] = e3;
+    return cnt;
+}
+
+// Bytes of packet a k_entropy CTA stages in shared memory: its 32 tiles are
+// contiguous in the packet, and a span this size covers tiles of up to 1 KB
+// on average. Larger spans are read from global memory instead.
+constexpr uint32_t kStageBytes = 32 * 1024;
+
+template <uint32_t LC>
+__global__ void __launch_bounds__(128) k_entropy(FrameDesc d, int greens, const uint32_t* __restrict__ tile_off,
+                                                 prr_dev_status* __restrict__ st) {
+    __shared__ CodeTables T;
+    __shared__ __align__(16) uint32_t stage[kStageBytes / 4];
+    load_tables(&T);
+    // The CTA's tiles [t0, t1) occupy bytes [tile_off[t0], tile_off[t1]).
+    const uint32_t t0 = blockIdx.x * (blockDim.x / 4);
+    const uint32_t t1 = min(t0 + blockDim.x / 4, d.ntiles);
+    const uint32_t hi = min(tile_off[t1], d.len);
+    const uint32_t lo = min(tile_off[t0], hi);
+    const uint32_t base = lo & ~15u, top = (hi + 15) & ~15u;  // within the padded packet buffer
+    const bool staged = top - base <= kStageBytes;
+    if (staged) {
+        const uint4* src = reinterpret_cast<const uint4*>(d.words) + base / 16;
+        uint4* dst = reinterpret_cast<uint4*>(stage);
+        for (uint32_t i = threadIdx.x; i < (top - base) / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    __syncthreads();
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= 4 * d.ntiles) return;
+    const uint32_t tile = g >> 2, s = g & 3;
+    if (LC != 6 && s == 1 && !greens) return;  // a reduced decode reads the second green only to average
+    const uint32_t trow = tile / d.tiles_per_row, j = tile - trow * d.tiles_per_row;
+    uint32_t x, log2;
+    tile_geom(j, d.columns, d.alignment, x, log2);
+    const uint32_t off = tile_off[tile], end = tile_off[tile + 1];
+    if (!(off <= end && end <= d.len) || end - off < 8) return;
+    const uint32_t size = end - off;
+    const uint32_t header_len = byte_at(d.words, off) >> 3;
+    const uint32_t qscale = byte_at(d.words, off + 1);
+    const uint32_t s0 = be16_at(d.words, off + 2), s1 = be16_at(d.words, off + 4), s2 = be16_at(d.words, off + 6);
+    const uint32_t used = header_len + s0 + s1 + s2;
+    if (!(header_len >= 8 && qscale != 0 && s0 != 0 && s1 != 0 && s2 != 0 && used < size)) return;
+    const uint32_t soff = off + header_len + (s > 0 ? s0 : 0) + (s > 1 ? s1 : 0) + (s > 2 ? s2 : 0);
+    const uint32_t slen = s == 0 ? s0 : s == 1 ? s1 : s == 2 ? s2 : size - used;
+    uint32_t* list = d.pairs + stream_list_base(d, trow, x, log2, s, LC);
+    bool revisited = false, ok = true;
+    const uint32_t cnt =
+        staged ? entropy_events<LC>(SharedWords{stage, base >> 2}, soff, slen, log2, T, list, revisited, ok)
+               : entropy_events<LC>(GlobalWords{d.words}, soff, slen, log2, T, list, revisited, ok);
+    if (!ok) atomicOr(&st->error, 1u);
+    d.counts[g] = revisited ? 0x80000000u : cnt;
+}
+
+// ---------------------------------------------------------------------------
 // Diagnostics: transforms of raw blocks, entropy decode of raw streams.
 __global__ void k_transform_blocks(int kind, const int16_t* __restrict__ coefs,
                                    const int16_t* __restrict__ q, uint16_t* __restrict__ out, size_t n) {
@@ -515,8 +738,9 @@ __global__ void k_decode_components(const uint32_t* __restrict__ words, const ui
     const uint32_t codes = 1u << (log2_blocks + log2_coefs);
     int16_t* dst = coefs + i * codes;
     for (uint32_t k = 0; k < codes; k++) dst[k] = 0;
-    decode_component(words, off[i], len[i], uint32_t(log2_blocks), uint32_t(log2_coefs), T,
-                     [&](uint32_t idx, int16_t v) { dst[idx] = v; });
+    bool revisited = false;
+    decode_component(GlobalWords{words}, off[i], len[i], uint32_t(log2_blocks), uint32_t(log2_coefs), T,
+                     [&](uint32_t idx, int16_t v) { dst[idx] = v; }, revisited);
 }
 
 // ---------------------------------------------------------------------------
@@ -558,26 +782,77 @@ cudaError_t launch_tile_index(const FrameDesc& d, uint32_t* tile_off, prr_dev_st
     return cudaGetLastError();
 }
 
-cudaError_t launch_decode_full(const FrameDesc& d, int idct, const uint32_t* tile_off, prr_dev_status* st,
-                               uint32_t* skipped, uint16_t* out, cudaStream_t s) {
-    dim3 grid(d.segs_per_row, d.tile_rows);
-    if (idct == PRR_IDCT_FFMPEG)
-        k_decode_full<PRR_IDCT_FFMPEG><<<grid, kThreads, 0, s>>>(d, tile_off, st, skipped, out);
+DecodeScratch decode_scratch_layout(uint32_t ntiles, uint32_t coded_w, uint32_t coded_h) {
+    auto up = [](size_t v) { return (v + 255) & ~size_t(255); };
+    DecodeScratch l;
+    l.tile_off = 0;
+    l.counts = up(4 * (size_t(ntiles) + 1));
+    l.pairs = l.counts + up(16 * size_t(ntiles));
+    l.total = l.pairs + up(4 * size_t(coded_w) * coded_h);
+    return l;
+}
+
+// The split path launches k_entropy first (128 threads per CTA: 32 tiles'
+// streams), then the transform kernel; the fused path only the latter.
+static cudaError_t launch_entropy(const FrameDesc& d, uint32_t lc, int greens, const uint32_t* tile_off,
+                                  prr_dev_status* st, cudaStream_t s) {
+    const unsigned blocks = unsigned((4 * size_t(d.ntiles) + 127) / 128);
+    if (lc == 6)
+        k_entropy<6><<<blocks, 128, 0, s>>>(d, greens, tile_off, st);
+    else if (lc == 4)
+        k_entropy<4><<<blocks, 128, 0, s>>>(d, greens, tile_off, st);
     else
-        k_decode_full<PRR_IDCT_APPLE><<<grid, kThreads, 0, s>>>(d, tile_off, st, skipped, out);
+        k_entropy<2><<<blocks, 128, 0, s>>>(d, greens, tile_off, st);
     count_launch();
     return cudaGetLastError();
 }
 
+cudaError_t launch_decode_full(const FrameDesc& d, int idct, const uint32_t* tile_off, prr_dev_status* st,
+                               uint32_t* skipped, uint16_t* out, cudaStream_t s) {
+    dim3 grid(d.segs_per_row, d.tile_rows);
+    const bool split = d.pairs != nullptr;
+    if (split) {
+        const cudaError_t e = launch_entropy(d, 6, 1, tile_off, st, s);
+        if (e != cudaSuccess) return e;
+    }
+    if (idct == PRR_IDCT_FFMPEG) {
+        if (split)
+            k_decode_full<PRR_IDCT_FFMPEG, true><<<grid, kThreads, 0, s>>>(d, tile_off, st, skipped, out);
+        else
+            k_decode_full<PRR_IDCT_FFMPEG, false><<<grid, kThreads, 0, s>>>(d, tile_off, st, skipped, out);
+    } else {
+        if (split)
+            k_decode_full<PRR_IDCT_APPLE, true><<<grid, kThreads, 0, s>>>(d, tile_off, st, skipped, out);
+        else
+            k_decode_full<PRR_IDCT_APPLE, false><<<grid, kThreads, 0, s>>>(d, tile_off, st, skipped, out);
+    }
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <int SHIFT>
+static void launch_reduced_t(const FrameDesc& d, int greens, const uint32_t* tile_off, prr_dev_status* st,
+                             uint32_t* skipped, uint16_t* out, cudaStream_t s) {
+    dim3 grid(d.segs_per_row, d.tile_rows);
+    if (d.pairs != nullptr)
+        k_decode_reduced<SHIFT, true><<<grid, kThreads, 0, s>>>(d, greens, tile_off, st, skipped, out);
+    else
+        k_decode_reduced<SHIFT, false><<<grid, kThreads, 0, s>>>(d, greens, tile_off, st, skipped, out);
+}
+
 cudaError_t launch_decode_reduced(const FrameDesc& d, int shift, int greens, const uint32_t* tile_off,
                                   prr_dev_status* st, uint32_t* skipped, uint16_t* out, cudaStream_t s) {
-    dim3 grid(d.segs_per_row, d.tile_rows);
+    if (d.pairs != nullptr) {
+        const uint32_t lc = shift == 1 ? 6 : (shift == 2 ? 4 : 2);
+        const cudaError_t e = launch_entropy(d, lc, greens, tile_off, st, s);
+        if (e != cudaSuccess) return e;
+    }
     if (shift == 1)
-        k_decode_reduced<1><<<grid, kThreads, 0, s>>>(d, greens, tile_off, st, skipped, out);
+        launch_reduced_t<1>(d, greens, tile_off, st, skipped, out, s);
     else if (shift == 2)
-        k_decode_reduced<2><<<grid, kThreads, 0, s>>>(d, greens, tile_off, st, skipped, out);
+        launch_reduced_t<2>(d, greens, tile_off, st, skipped, out, s);
     else
-        k_decode_reduced<3><<<grid, kThreads, 0, s>>>(d, greens, tile_off, st, skipped, out);
+        launch_reduced_t<3>(d, greens, tile_off, st, skipped, out, s);
     count_launch();
     return cudaGetLastError();
 }

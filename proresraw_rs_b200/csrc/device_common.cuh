@@ -85,13 +85,36 @@ __device__ __forceinline__ uint32_t be16_at(const uint32_t* __restrict__ words, 
     return (byte_at(words, p) << 8) | byte_at(words, p + 1);
 }
 
+// Word sources of the bit reader: the packet in global memory, or a copy of
+// a span of it in shared memory (words `base` onwards), indexed by the
+// packet's word index either way.
+struct GlobalWords {
+    const uint32_t* w;
+    __device__ __forceinline__ uint32_t operator()(uint32_t i) const { return __ldg(w + i); }
+};
+struct SharedWords {
+    const uint32_t* w;
+    uint32_t base;
+    __device__ __forceinline__ uint32_t operator()(uint32_t i) const { return w[i - base]; }
+};
+
+template <class Src>
+__device__ __forceinline__ uint32_t be_bytes_src(const Src& src, uint32_t p, uint32_t n) {
+    if (n == 0) return 0;
+    const uint32_t sh = (p & 3) * 8;
+    uint32_t v = bswap32(src(p >> 2)) << sh;
+    if ((p & 3) + n > 4) v |= bswap32(src((p >> 2) + 1)) >> (32 - sh);
+    return v & (0xFFFFFFFFu << (32 - 8 * n));
+}
+
 // ---------------------------------------------------------------------------
 // Bit reader, src/bits.rs:17-112: a 64-bit window whose top 32 bits are the
 // view, a signed count of valid bits below it, one aligned big-endian word
-// per refill, zero fill past the end. The next refill word is loaded one
-// refill ahead so its latency hides behind the symbols in between.
+// per refill, zero fill past the end. The next refill word is fetched one
+// refill ahead and touched only by the next refill.
+template <class Src>
 struct Reader {
-    const uint32_t* words;
+    Src src;
     uint32_t words_end;  // whole words may be loaded while pos < words_end
     uint32_t end;        // one past the stream's last byte (packet offsets)
     uint32_t nxt;        // the value the next refill returns
@@ -101,10 +124,10 @@ struct Reader {
 
     __device__ __forceinline__ void peek(uint32_t p) {
         if (p < words_end) {
-            nxt = bswap32(__ldg(words + (p >> 2)));
+            nxt = bswap32(src(p >> 2));
             nxt_pos = p + 4;
         } else {
-            nxt = be_bytes(words, p, end - p);
+            nxt = be_bytes_src(src, p, end - p);
             nxt_pos = end;
         }
     }
@@ -112,18 +135,18 @@ struct Reader {
     // BitReader::new (src/bits.rs:295-327) for `len` bytes at packet offset
     // `off`; the stream's alignment is off & 3 (the packet counts as aligned,
     // src/decoder.rs:288-291).
-    __device__ __forceinline__ void init(const uint32_t* w, uint32_t off, uint32_t len) {
-        words = w;
+    __device__ __forceinline__ void init(const Src& s, uint32_t off, uint32_t len) {
+        src = s;
         end = off + len;
         uint32_t remaining = len;
         uint32_t pos;
         uint32_t first;
         if (remaining < 4) {
-            first = be_bytes(w, off, remaining);
+            first = be_bytes_src(src, off, remaining);
             pos = off + remaining;
             remaining = 0;
         } else {
-            first = be_bytes(w, off, 4);
+            first = be_bytes_src(src, off, 4);
             pos = off + 4;
             remaining -= 4;
         }
@@ -131,7 +154,7 @@ struct Reader {
         extra = 0;
         const uint32_t to_boundary = (4 - (pos & 3)) & 3;
         if (to_boundary != 0 && to_boundary <= remaining) {
-            low = be_bytes(w, pos, to_boundary);
+            low = be_bytes_src(src, pos, to_boundary);
             pos += to_boundary;
             remaining -= to_boundary;
             extra = int32_t(8 * to_boundary);
@@ -143,7 +166,8 @@ struct Reader {
 
     __device__ __forceinline__ uint32_t top() const { return uint32_t(window >> 32); }
 
-    // BitReader::consume (src/bits.rs:348-356).
+    // BitReader::consume (src/bits.rs:348-356): drop n bits, refilling at
+    // most once.
     __device__ __forceinline__ void consume(uint32_t n) {
         window <<= (n & 63);
         extra = int32_t(uint32_t(extra) - n);
@@ -156,107 +180,110 @@ struct Reader {
     }
 };
 
-// codeword, src/bits.rs:367-385. p != 0.
+// codeword, src/bits.rs:367-385, for a view p != 0: value and length. The
+// Rice and exp-Golomb results are both computed and one is selected, so
+// lanes decoding different kinds of codeword do not diverge. (The crate's
+// separate branch for a set top bit is the Rice case with no leading zero.)
 __device__ __forceinline__ uint32_t codeword(uint32_t p, uint32_t cb, uint32_t& len) {
     const uint32_t r = cb & 15;
-    if (int32_t(p) < 0) {
-        len = r + 1;
-        return (p & 0x7fffffffu) >> ((31u - r) & 31);
-    }
-    const uint32_t lz = __clz(p);
     const uint32_t s = cb >> 8;
-    if (lz <= s) {
-        len = r + 1 + lz;
-        return (lz << r) + (((p << ((lz + 1) & 31)) >> 1) >> ((31u - r) & 31));
-    }
     const uint32_t e = (cb >> 4) & 15;
-    len = 2 * lz - s + e;
-    return ((s + 1) << r) + (p >> ((32u - len) & 31)) - (1u << e);
+    const uint32_t lz = __clz(p);
+    const uint32_t rice_len = r + 1 + lz;
+    const uint32_t rice_val = (lz << r) + (((p << ((lz + 1) & 31)) >> 1) >> ((31u - r) & 31));
+    const uint32_t eg_len = 2 * lz - s + e;
+    const uint32_t eg_val = ((s + 1) << r) + (p >> ((32u - eg_len) & 31)) - (1u << e);
+    const bool rice = lz <= s;
+    len = rice ? rice_len : eg_len;
+    return rice ? rice_val : eg_val;
 }
 
-// decode_component_reduced, src/coefficients.rs:203-312. The destination
-// must hold zeros; `store(index, value)` receives each coefficient written,
-// index = block * (1 << log2_coefs) + position within the block's corner.
-// A wrapped zero run may revisit an index: the later store wins, as on the
-// host. Returns false if the loop bound was hit (not reachable by any stream
-// of `len` bytes; kept so that every device loop is bounded).
-template <class Store>
-__device__ __forceinline__ bool decode_component(const uint32_t* words, uint32_t off, uint32_t len,
+// decode_component_reduced, src/coefficients.rs:203-312, as a state machine
+// that decodes one symbol per iteration: the DC fold, the DC deltas, the
+// non-zero run length, the levels of a run, the zero run and the level after
+// it. Every lane of a warp runs the same codeword and consume for its own
+// stream, whatever state its stream is in; only the short per-state updates
+// differ. The destination must hold zeros; `store(index, value)` receives
+// each coefficient written, index = block * (1 << log2_coefs) + position
+// within the block's corner. A wrapped zero run may revisit an index (the
+// later store wins, as on the host) and sets `revisited`. Returns false if
+// the iteration bound was hit, which no stream of `len` bytes reaches: every
+// symbol shifts the window or moves the reader a word on.
+template <class Src, class Store>
+__device__ __forceinline__ bool decode_component(const Src& src, uint32_t off, uint32_t len,
                                                  uint32_t log2_blocks, uint32_t log2_coefs,
-                                                 const CodeTables& T, Store store) {
+                                                 const CodeTables& T, Store store, bool& revisited) {
+    enum : uint32_t { FIRST, DC, RUN_LENGTH, LEVELS, ZEROS, LEVEL, };
     const uint8_t* scan = log2_coefs == 6 ? T.scan : (log2_coefs == 4 ? T.scan4 : T.scan2);
     const uint32_t blocks = 1u << log2_blocks;
     const uint32_t codes = blocks << log2_coefs;
     const uint32_t block_mask = blocks - 1;
-    Reader r;
-    r.init(words, off, len);
-    if (r.top() == 0) return true;
-    uint32_t l;
-    const uint32_t first = codeword(r.top(), FIRST_DC, l);
-    r.consume(l);
-    const uint32_t odd = first & 1;
-    int32_t dc = int32_t((((odd + first) >> 1) ^ (0u - odd)) + odd);
-    store(0u, int16_t(dc));
-    uint32_t dc_cb = DC_RESET;
-    uint32_t sign = 0;
-    for (uint32_t block = 1; block < blocks; block++) {
-        if (r.top() == 0) return true;
-        const uint32_t symbol = codeword(r.top(), dc_cb, l);
-        sign ^= symbol & 1;
-        const uint32_t magnitude = ((symbol & 1) + symbol) >> 1;
-        const int32_t delta = int32_t(((0u - sign) ^ magnitude) + sign);
-        dc_cb = T.dc[min(magnitude, 12u)];
-        sign = delta < 0 ? 1u : 0u;
-        r.consume(l);
-        dc = int32_t(uint32_t(dc) + uint32_t(delta));
-        store(block << log2_coefs, int16_t(dc));
-    }
+    Reader<Src> r;
+    r.init(src, off, len);
+    uint32_t state = FIRST, cb = FIRST_DC;
+    int32_t dc = 0;
+    uint32_t sign = 0, block = 1;
     uint32_t ac_cb = AC_INITIAL, rn_cb = RN_INITIAL, ln_cb = LN_INITIAL;
-    uint32_t n = blocks;
-    if (n >= codes) return true;
-    // Each iteration consumes at least one bit of the window or moves the
-    // reader a word on; 64 iterations per stream bit bounds any stream.
+    uint32_t n = blocks, run = 0;
     uint32_t budget = 64u * (8u * len + 64u) + 4u * codes;
-    auto level = [&](uint32_t cb, uint32_t& symbol) -> int16_t {
+    for (;;) {
         const uint32_t top = r.top();
-        uint32_t ln;
-        symbol = codeword(top, cb, ln);
-        const bool negative = int32_t(top << (ln & 31)) < 0;
-        r.consume(ln + 1);
-        const uint16_t mag = uint16_t(uint16_t(symbol) + 1);
-        return int16_t(negative ? uint16_t(0u - mag) : mag);
-    };
-    auto place = [&](uint32_t k) -> uint32_t {
-        return uint32_t(scan[k >> log2_blocks]) + ((k & block_mask) << log2_coefs);
-    };
-    while (r.top() != 0) {
+        if (top == 0) return true;  // end of component: the rest stays zero
         if (budget-- == 0) return false;
-        const uint32_t run = codeword(r.top(), ln_cb, l);
-        r.consume(l);
-        for (uint32_t i = 0; i < run; i++) {
-            if (r.top() == 0) return true;
-            uint32_t symbol;
-            const int16_t v = level(ac_cb, symbol);
-            ac_cb = T.ac[min(symbol, 94u)];
-            store(place(n), v);
+        uint32_t l;
+        const uint32_t v = codeword(top, cb, l);
+        const bool is_level = state == LEVELS || state == LEVEL;
+        // A level's sign is the bit after its codeword (src/coefficients.rs:256-270).
+        const bool negative = int32_t(top << (l & 31)) < 0;
+        r.consume(l + (is_level ? 1u : 0u));
+        if (is_level) {
+            const uint16_t mag = uint16_t(uint16_t(v) + 1);
+            const int16_t value = int16_t(negative ? uint16_t(0u - mag) : mag);
+            ac_cb = T.ac[min(v, 94u)];
+            store(uint32_t(scan[n >> log2_blocks]) + ((n & block_mask) << log2_coefs), value);
             n += 1;
-            if (n == codes) return true;
+            if (state == LEVEL) {
+                ln_cb = T.ln[min(v, 14u)];
+                if (n >= codes) return true;
+                state = RUN_LENGTH;
+                cb = ln_cb;
+            } else {
+                if (n == codes) return true;
+                run -= 1;
+                state = run == 0 ? ZEROS : LEVELS;
+                cb = run == 0 ? rn_cb : ac_cb;
+            }
+        } else if (state == RUN_LENGTH) {
+            run = v;
+            state = run > 0 ? LEVELS : ZEROS;
+            cb = run > 0 ? ac_cb : rn_cb;
+        } else if (state == ZEROS) {
+            rn_cb = T.rn[min(v, 27u)];
+            const uint32_t before = n;
+            n = n + 1 + v;  // a zero run is zeros + 1 long; wraps like the crate's u32
+            if (n < before) revisited = true;
+            if (n >= codes) return true;
+            state = LEVEL;
+            cb = ac_cb;
+        } else if (state == DC) {
+            sign ^= v & 1;
+            const uint32_t magnitude = ((v & 1) + v) >> 1;
+            const int32_t delta = int32_t(((0u - sign) ^ magnitude) + sign);
+            sign = delta < 0 ? 1u : 0u;
+            dc = int32_t(uint32_t(dc) + uint32_t(delta));
+            store(block << log2_coefs, int16_t(dc));
+            block += 1;
+            const uint32_t next_dc = T.dc[min(magnitude, 12u)];
+            state = block == blocks ? RUN_LENGTH : DC;
+            cb = block == blocks ? ln_cb : next_dc;
+        } else {  // FIRST: the sign-folded first DC
+            const uint32_t odd = v & 1;
+            dc = int32_t((((odd + v) >> 1) ^ (0u - odd)) + odd);
+            store(0u, int16_t(dc));
+            state = blocks > 1 ? DC : RUN_LENGTH;
+            cb = blocks > 1 ? uint32_t(DC_RESET) : ln_cb;
         }
-        if (r.top() == 0) return true;
-        const uint32_t zeros = codeword(r.top(), rn_cb, l);
-        rn_cb = T.rn[min(zeros, 27u)];
-        r.consume(l);
-        n = n + 1 + zeros;
-        if (n >= codes || r.top() == 0) return true;
-        uint32_t symbol;
-        const int16_t v = level(ac_cb, symbol);
-        ac_cb = T.ac[min(symbol, 94u)];
-        ln_cb = T.ln[min(symbol, 14u)];
-        store(place(n), v);
-        n += 1;
-        if (n >= codes) return true;
     }
-    return true;
 }
 
 // dequantize, src/idct.rs:41-43: 32-bit product saturated to 16 bits.

@@ -24,7 +24,19 @@ struct FrameDesc {
     uint32_t curve_c0[8];   // linearization segments (reduced decode)
     uint32_t curve_delta[8];
     uint8_t qmat[64];
+    // Split decode (k_entropy, then the transform kernel): per-stream entry
+    // counts and (position, value) lists. Both null: the fused kernels
+    // entropy-decode inside the transform CTA.
+    uint32_t* counts;
+    uint32_t* pairs;
 };
+
+// Scratch of the split decode for a frame: tile offsets, then per-stream
+// counts, then the coefficient lists, each 256-byte aligned.
+struct DecodeScratch {
+    size_t tile_off, counts, pairs, total;
+};
+DecodeScratch decode_scratch_layout(uint32_t ntiles, uint32_t coded_w, uint32_t coded_h);
 
 FrameDesc make_frame_desc(const prr_frame_info& info, const uint8_t* dev_packet);
 
