@@ -218,8 +218,15 @@ def run(args):
     info0 = infos[0]
     n = W * H
     torch.cuda.synchronize()
-    stream = torch.cuda.current_stream()
-    ctx = P.context()
+    # One stream: decode then develop, frame after frame. (Decoding frame k+1
+    # on a second stream while frame k develops was measured slower: the
+    # latency-bound entropy warps lose issue slots to the develop kernel.)
+    s_dec = torch.cuda.Stream()
+    s_dev = s_dec
+    dev_index = torch.cuda.current_device()
+    ctx_dec = C.c_void_p()
+    assert L.prr_ctx_create(dev_index, C.c_void_p(s_dec.cuda_stream), C.byref(ctx_dec)) == 0
+    ctx_dev = ctx_dec
 
     # Device-resident packets (padded), scratch, outputs.
     dpk = []
@@ -227,7 +234,8 @@ def run(args):
         buf = torch.zeros(L.prr_padded_packet_bytes(len(p)), dtype=torch.uint8, device="cuda")
         buf[: len(p)].copy_(torch.frombuffer(bytearray(p), dtype=torch.uint8))
         dpk.append(buf)
-    samples = torch.empty(info0.coded_width * info0.coded_height, dtype=torch.uint16, device="cuda")
+    samples = [torch.empty(info0.coded_width * info0.coded_height, dtype=torch.uint16, device="cuda")
+               for _ in range(2)]
     status = torch.zeros(4 * RING, dtype=torch.int32, device="cuda")
     skipped = torch.zeros(info0.ntiles * RING, dtype=torch.int32, device="cuda")
     nscr = L.prr_decode_scratch_bytes(C.byref(info0))
@@ -243,21 +251,32 @@ def run(args):
         hdrs.append(pf.header)
         params.append(P.DemosaicParams.new(pf.header, P.frame_quantizer(pf))._c())
 
+    dec_done = [torch.cuda.Event() for _ in range(2)]
+    dev_done = [torch.cuda.Event() for _ in range(2)]
+
     def step(k, ev=None):
-        i = k % RING
+        i, buf = k % RING, k % 2
+        # Decode frame k into code buffer k % 2 once develop k - 2 has read it.
+        if k >= 2:
+            s_dec.wait_event(dev_done[buf])
         if ev:
-            ev[0].record(stream)
-        rc = L.prr_decode_async(ctx, C.byref(infos[i]), dpk[i].data_ptr(), 0, samples.data_ptr(),
+            ev[0].record(s_dec)
+        rc = L.prr_decode_async(ctx_dec, C.byref(infos[i]), dpk[i].data_ptr(), 0, samples[buf].data_ptr(),
                                 status.data_ptr() + 16 * i, skipped.data_ptr() + 4 * info0.ntiles * i,
                                 scratch.data_ptr(), nscr)
         assert rc == 0, rc
         if ev:
-            ev[1].record(stream)
-        rc = L.prr_develop(ctx, C.byref(hdrs[i]._c), C.byref(params[i]), 2, samples.data_ptr(), 1,
+            ev[1].record(s_dec)
+        dec_done[buf].record(s_dec)
+        s_dev.wait_event(dec_done[buf])
+        if ev:
+            ev[2].record(s_dev)
+        rc = L.prr_develop(ctx_dev, C.byref(hdrs[i]._c), C.byref(params[i]), 2, samples[buf].data_ptr(), 1,
                            r.data_ptr(), g.data_ptr(), b.data_ptr(), n)
         assert rc == 0, rc
         if ev:
-            ev[2].record(stream)
+            ev[3].record(s_dev)
+        dev_done[buf].record(s_dev)
 
     for k in range(max(3, args.warmup)):
         step(k)
@@ -265,24 +284,26 @@ def run(args):
     st = status.cpu().numpy().view(np.uint32).reshape(RING, 4)
     assert np.all(st[:, 0] == 0xFFFFFFFF) and np.all(st[:, 3] == 0)
 
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     launches0 = L.prr_kernel_launches()
     with Clocks(torch.cuda.current_device()) as clocks:
-        start.record(stream)
+        start.record(s_dec)
         for k in range(args.steps):
             step(k, evs[k])
-        end.record(stream)
+        end.record(s_dev)
         torch.cuda.synchronize()
     launches = L.prr_kernel_launches() - launches0
     if world > 1:
         torch.distributed.barrier()
     ms = start.elapsed_time(end)
+    # Per-kernel durations, events on the stream the kernels run on.
     dec_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps
-    dev_ms = sum(e[1].elapsed_time(e[2]) for e in evs) / args.steps
+    dev_ms = sum(e[2].elapsed_time(e[3]) for e in evs) / args.steps
+    L.prr_ctx_destroy(ctx_dec)
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)

@@ -528,9 +528,131 @@ __global__ void __launch_bounds__(kThreads) k_decode_reduced(FrameDesc d, int gr
 // The symbol loop is decode_component_reduced (src/coefficients.rs:203-312)
 // as a state machine, one symbol per iteration; the codebook lookups of all
 // states are issued together and the state's own update picks its result.
+// The 25 distinct codebook parameter sets of the format (src/codebook.rs:25-55).
+// The entropy kernel names a codebook by its index here.
+constexpr int kCodebooks = 25;
+__constant__ uint16_t c_cb_params[kCodebooks] = {0x2BC, 0x064, 0x010, 0x021, 0x032, 0x033, 0x044,
+                                                 0x076, 0x031, 0x000, 0x211, 0x111, 0x222, 0x122,
+                                                 0x233, 0x133, 0x244, 0x355, 0x166, 0x200, 0x100,
+                                                 0x011, 0x022, 0x042, 0x433};
+constexpr uint32_t kIdFirstDc = 0, kIdDcReset = 1, kIdAcInitial = 8, kIdRnInitial = 9, kIdLnInitial = 23;
+
+// Codeword decoding by table. For a view p with lz leading zeros, codeword()
+// (src/bits.rs:367-385) is value = base + ((p << sh1) >> sh2) with a shift of
+// 32 giving 0, and a length, all fixed by (codebook, lz):
+//   Rice (lz <= s):  base = lz << r, sh1 = (lz + 1) & 31, sh2 = 32 - r,
+//                    length r + 1 + lz;
+//   exp-Golomb:      base = ((s + 1) << r) - (1 << e), sh1 = 0,
+//                    sh2 = (32 - length) & 31, length 2 lz - s + e,
+// in wrapping u32 arithmetic, over-long codewords included. One shared
+// load replaces the arithmetic of the symbol loop's critical chain.
+struct EntropyTables {
+    uint2 cw[kCodebooks * 32];  // x: base, y: length | sh1 << 8 | sh2 << 16
+    uint8_t ac[96], rn[32], ln[16], dc[16];  // next codebook index, by clamped symbol
+};
+
+__device__ __forceinline__ void build_entropy_tables(EntropyTables& E, const CodeTables& T) {
+    auto id_of = [](uint32_t params) {
+        uint32_t id = 0;
+        for (int k = 0; k < kCodebooks; k++)
+            if (c_cb_params[k] == params) id = uint32_t(k);
+        return id;
+    };
+    for (uint32_t i = threadIdx.x; i < kCodebooks * 32; i += blockDim.x) {
+        const uint32_t p = c_cb_params[i >> 5], lz = i & 31;
+        const uint32_t s = p >> 8, e = (p >> 4) & 15, r = p & 15;
+        uint32_t base, len, sh1, sh2;
+        if (lz <= s) {
+            base = lz << r;
+            len = r + 1 + lz;
+            sh1 = (lz + 1) & 31;
+            sh2 = 32 - r;
+        } else {
+            len = 2 * lz - s + e;
+            base = ((s + 1) << r) - (1u << e);
+            sh1 = 0;
+            sh2 = (32u - len) & 31;
+        }
+        E.cw[i] = make_uint2(base, len | (sh1 << 8) | (sh2 << 16));
+    }
+    for (uint32_t i = threadIdx.x; i < 95; i += blockDim.x) E.ac[i] = uint8_t(id_of(T.ac[i]));
+    for (uint32_t i = threadIdx.x; i < 28; i += blockDim.x) E.rn[i] = uint8_t(id_of(T.rn[i]));
+    for (uint32_t i = threadIdx.x; i < 15; i += blockDim.x) E.ln[i] = uint8_t(id_of(T.ln[i]));
+    for (uint32_t i = threadIdx.x; i < 13; i += blockDim.x) E.dc[i] = uint8_t(id_of(T.dc[i]));
+}
+
+// The bit reader of src/bits.rs:17-112 with a refill that every lane runs
+// on every symbol, so that the refills of different lanes do not split the
+// warp. The word a refill would load is computed from the byte position
+// alone: n = min(4, end - pos) bytes at pos, big-endian, zero-filled, and pos
+// advances by n. That equals BitReader::next_word: whole words while four
+// bytes remain, then the partial tail, then zeros (pos is 4-aligned whenever
+// four bytes remain, so words_end need not be kept). It is ORed into the
+// window only when the count of bits below the view goes negative, exactly
+// as consume() does. Loads may touch the word after the stream's last byte,
+// which both word sources provide (padded packet, padded stage).
+template <class Src>
+struct LeanReader {
+    Src src;
+    uint32_t pos, end;
+    uint64_t window;
+    int32_t extra;
+
+    __device__ __forceinline__ uint32_t word_at(uint32_t p) const {
+        const uint32_t k = p >> 2;
+        const uint32_t hi = bswap32(src(k)), lo = bswap32(src(k + 1));
+        const uint32_t w = __funnelshift_l(lo, hi, (p & 3) * 8);
+        const uint32_t n = min(4u, end - min(p, end));
+        return n == 0 ? 0u : (w & (0xFFFFFFFFu << (32 - 8 * n)));
+    }
+
+    __device__ __forceinline__ void init(const Src& s, uint32_t off, uint32_t len) {
+        // BitReader::new (src/bits.rs:295-327).
+        src = s;
+        end = off + len;
+        uint32_t remaining = len;
+        const uint32_t first = word_at(off);
+        const uint32_t took = min(4u, remaining);
+        pos = off + took;
+        remaining -= took;
+        uint32_t low = 0;
+        extra = 0;
+        const uint32_t to_boundary = (4 - (pos & 3)) & 3;
+        if (to_boundary != 0 && to_boundary <= remaining) {
+            low = word_at(pos) & (0xFFFFFFFFu << (32 - 8 * to_boundary));
+            pos += to_boundary;
+            extra = int32_t(8 * to_boundary);
+        }
+        window = (uint64_t(first) << 32) | uint64_t(low);
+    }
+
+    __device__ __forceinline__ uint32_t top() const { return uint32_t(window >> 32); }
+
+    // BitReader::consume (src/bits.rs:348-356).
+    __device__ __forceinline__ void consume(uint32_t n) {
+        const uint32_t w = word_at(pos);  // independent of n: issued early
+        window <<= (n & 63);
+        extra = int32_t(uint32_t(extra) - n);
+        const bool refill = extra < 0;
+        const uint32_t shift = uint32_t(-int32_t(int8_t(extra))) & 63;
+        window |= refill ? (uint64_t(w) << shift) : 0ull;
+        const uint32_t adv = min(4u, end - min(pos, end));
+        pos += refill ? adv : 0u;
+        extra += refill ? 32 : 0;
+    }
+};
+
+// codeword() through the table: value, and the length in `len`.
+__device__ __forceinline__ uint32_t table_codeword(const EntropyTables& E, uint32_t top, uint32_t cb,
+                                                   uint32_t& len) {
+    const uint2 ce = E.cw[(cb << 5) | __clz(top)];
+    len = ce.y & 0xFF;
+    return ce.x + __funnelshift_rc(top << ((ce.y >> 8) & 0xFF), 0u, ce.y >> 16);
+}
+
 template <uint32_t LC, class Src>
 __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off, uint32_t len,
-                                                   uint32_t log2_blocks, const CodeTables& T, uint32_t* list,
+                                                   uint32_t log2_blocks, const EntropyTables& T, uint32_t* list,
                                                    bool& revisited, bool& ok) {
     const uint32_t blocks = 1u << log2_blocks;
     const uint32_t codes = blocks << LC;
@@ -551,18 +673,18 @@ __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off,
     // (src/coefficients.rs:225-248).
     if (live) {
         uint32_t l;
-        const uint32_t v = codeword(r.top(), FIRST_DC, l);
+        const uint32_t v = table_codeword(T, r.top(), kIdFirstDc, l);
         r.consume(l);
         const uint32_t odd = v & 1;
         int32_t dc = int32_t((((odd + v) >> 1) ^ (0u - odd)) + odd);
         append(0, uint32_t(dc));
-        uint32_t dc_cb = DC_RESET, sign = 0;
+        uint32_t dc_cb = kIdDcReset, sign = 0;
         for (uint32_t block = 1; block < blocks; block++) {
             if (r.top() == 0) {
                 live = false;
                 break;
             }
-            const uint32_t s = codeword(r.top(), dc_cb, l);
+            const uint32_t s = table_codeword(T, r.top(), dc_cb, l);
             sign ^= s & 1;
             const uint32_t magnitude = ((s & 1) + s) >> 1;
             const int32_t delta = int32_t(((0u - sign) ^ magnitude) + sign);
@@ -578,8 +700,8 @@ __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off,
     // length of a non-zero run, a level inside the run, a zero run, the level
     // after a zero run.
     enum : uint32_t { RUN_LENGTH = 0, ZEROS = 1, LEVELS = 2, LEVEL = 3 };
-    uint32_t state = RUN_LENGTH, cb = LN_INITIAL;
-    uint32_t ac_cb = AC_INITIAL, rn_cb = RN_INITIAL, ln_cb = LN_INITIAL;
+    uint32_t state = RUN_LENGTH, cb = kIdLnInitial;
+    uint32_t ac_cb = kIdAcInitial, rn_cb = kIdRnInitial, ln_cb = kIdLnInitial;
     uint32_t n = blocks, run = 0;
     uint32_t budget = 64u * (8u * len + 64u) + 4u * codes;
     while (live) {
@@ -590,7 +712,7 @@ __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off,
             break;
         }
         uint32_t l;
-        const uint32_t v = codeword(top, cb, l);
+        const uint32_t v = table_codeword(T, top, cb, l);
         const bool is_level = state >= LEVELS;
         const bool negative = int32_t(top << (l & 31)) < 0;
         r.consume(l + (is_level ? 1u : 0u));
@@ -630,9 +752,12 @@ constexpr uint32_t kStageBytes = 32 * 1024;
 template <uint32_t LC>
 __global__ void __launch_bounds__(128) k_entropy(FrameDesc d, int greens, const uint32_t* __restrict__ tile_off,
                                                  prr_dev_status* __restrict__ st) {
-    __shared__ CodeTables T;
-    __shared__ __align__(16) uint32_t stage[kStageBytes / 4];
-    load_tables(&T);
+    __shared__ CodeTables CT;
+    __shared__ EntropyTables T;
+    __shared__ __align__(16) uint32_t stage[kStageBytes / 4 + 4];  // + the word after the last byte
+    load_tables(&CT);
+    __syncthreads();
+    build_entropy_tables(T, CT);
     // The CTA's tiles [t0, t1) occupy bytes [tile_off[t0], tile_off[t1]).
     const uint32_t t0 = blockIdx.x * (blockDim.x / 4);
     const uint32_t t1 = min(t0 + blockDim.x / 4, d.ntiles);

@@ -96,6 +96,33 @@ __device__ __forceinline__ float estimate(const float* xx, const float* gg, cons
     return fma_(sub(mean_mid, mean_x), weight, mean_x);
 }
 
+// estimate() with lanes (u, v, u, v): two opposite neighbours each counted
+// twice (src/demosaic.rs:674-678). Each distinct lane is computed once; the
+// sums keep the four-lane order of dot4, so the result is estimate()'s.
+__device__ __forceinline__ float estimate2(float xu, float xv, float gu, float gv, float vu, float vv,
+                                           float su, float sv, float tu, float tv, float cg, float cs) {
+    const float mean_x = fma_(xv, 0.25f, fma_(xu, 0.25f, fma_(xu, 0.25f, mul(xv, 0.25f))));
+    if (!(cs < cg)) return mean_x;
+    if (!((su < xu) & (tu < gu) & (sv < xv) & (tv < gv))) return mean_x;
+    const float lo_u = dv(mul(sub(cg, cs), sub(xu, su)), add(tu, gu));
+    const float lo_v = dv(mul(sub(cg, cs), sub(xv, sv)), add(tv, gv));
+    const float mid_u = dv(mul(cg, xu), gu);
+    const float mid_v = dv(mul(cg, xv), gv);
+    const float hi_u = dv(mul(add(cs, cg), add(su, xu)), sub(gu, tu));
+    const float hi_v = dv(mul(add(cs, cg), add(sv, xv)), sub(gv, tv));
+    const float ml_u = sub(mid_u, lo_u), ml_v = sub(mid_v, lo_v);
+    const float hm_u = sub(hi_u, mid_u), hm_v = sub(hi_v, mid_v);
+    const float spread = fma_(ml_v, hm_v, fma_(ml_u, hm_u, fma_(ml_u, hm_u, mul(ml_v, hm_v))));
+    const float mean_mid = fma_(mid_v, 0.25f, fma_(mid_u, 0.25f, fma_(mid_u, 0.25f, mul(mid_v, 0.25f))));
+    const float dm_u = sub(mid_u, mean_mid), dm_v = sub(mid_v, mean_mid);
+    const float b = fma_(spread, 0.75f, fma_(dm_v, dm_v, fma_(dm_u, dm_u, fma_(dm_u, dm_u, mul(dm_v, dm_v)))));
+    const float dx_u = sub(xu, mean_x), dx_v = sub(xv, mean_x);
+    const float vsum = fma_(vv, 1.0f, fma_(vu, 1.0f, fma_(vu, 1.0f, mul(vv, 1.0f))));
+    const float a = fma_(vsum, 0.75f, fma_(dx_v, dx_v, fma_(dx_u, dx_u, fma_(dx_u, dx_u, mul(dx_v, dx_v)))));
+    const float weight = dv(a, add(b, a));
+    return fma_(sub(mean_mid, mean_x), weight, mean_x);
+}
+
 constexpr int TW = 32, TH = 32;           // output tile
 constexpr int NW = TW + 6, NH = TH + 6;   // normalized values, 3-sensel halo
 constexpr int GW = TW + 2, GH = TH + 2;   // green-pass region, 1-sensel halo
@@ -103,6 +130,12 @@ constexpr int kDevThreads = 256;          // one thread per 2x2 quad of the tile
 
 struct DevShared {
     float nrm[NH][NW];
+    // Green-pass noise terms of every normalized value once clipped at its
+    // own site's limit (1 at green sites, 1/gain at red and blue sites):
+    // variance with the green-pass offset, and its square root. The green
+    // pass needs them for each neighbour of every red or blue site.
+    float gvar[NH][NW];
+    float gsd[NH][NW];
     float rb[GH][GW];   // red or blue (0 at green sites)
     float gr[GH][GW];   // green
     float vx[GH][GW];   // variance(rb) with the chroma offset (red/blue sites)
@@ -113,6 +146,14 @@ struct DevShared {
 
 }  // namespace
 
+// PRE: the green pass reads the per-sensel noise terms staged in shared
+// memory instead of evaluating them for each neighbour. Valid when width and
+// height are both at least 4: every neighbour the green pass reads past a
+// picture edge is then replaced by mirror() (src/demosaic.rs:547-557), so
+// each neighbour slot holds a sensel of the site type the slot's clip limit
+// assumes (green at distance 1, the centre's colour at distance 2). Frames 2
+// sensels wide or tall keep the direct evaluation.
+template <bool PRE>
 __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
     __shared__ DevShared S;
     const int tid = threadIdx.x;
@@ -123,6 +164,8 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
         S.cd[tid] = d.curve_delta[tid];
     }
     __syncthreads();
+    const Noise nz{d.noise[0], d.noise[1], d.noise[2]};
+    const int red_row = d.cfa >> 1, red_col = d.cfa & 1;
     // 1. Normalized values, coordinates clamped to the picture as the green
     //    pass clamps them (src/demosaic.rs:370-375, 499).
     for (int i = tid; i < NH * NW; i += kDevThreads) {
@@ -131,11 +174,18 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
         const int x = min(max(x0 - 3 + tx, 0), w - 1);
         const uint32_t code = __ldg(d.codes + size_t(y) * d.stride + x);
         const int32_t lin = int32_t(curve_apply(S.c0, S.cd, code));
-        S.nrm[ty][tx] = mul(d.one_over_range, __int2float_rn(lin - d.black));
+        const float v = mul(d.one_over_range, __int2float_rn(lin - d.black));
+        S.nrm[ty][tx] = v;
+        if (PRE) {
+            const bool red_line = (y & 1) == red_row;
+            const bool rb = (x & 1) == (red_line ? red_col : 1 - red_col);
+            const float lim = rb ? (red_line ? d.clip[0] : d.clip[1]) : 1.0f;
+            const float var = variance(fminf(v, lim), d.green_off, nz);
+            S.gvar[ty][tx] = var;
+            S.gsd[ty][tx] = rt(var);
+        }
     }
     __syncthreads();
-    const Noise nz{d.noise[0], d.noise[1], d.noise[2]};
-    const int red_row = d.cfa >> 1, red_col = d.cfa & 1;
     // 2. Green pass on the region: red/blue sites first (the heavy ones),
     //    17 per region row, then green sites.
     for (int k = tid; k < GH * (GW / 2) * 2; k += kDevThreads) {
@@ -162,25 +212,45 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
                            fminf(S.nrm[ty - 2][tx], clip), fminf(S.nrm[ty + 2][tx], clip)};
             mirror(hh, x, w, c);
             mirror(vv, y, h, c);
-            float var_h[4], var_v[4];
+            float var_h[4], var_v[4], sd_h[4], sd_v[4];
+            float sdc;
+            if (PRE) {
+                // The same neighbours' precomputed terms, permuted by the
+                // same mirror() with the centre's terms standing for c.
+                const float vc = S.gvar[ty][tx];
+                sdc = S.gsd[ty][tx];
+                var_h[0] = S.gvar[ty][tx - 1]; var_h[1] = S.gvar[ty][tx + 1];
+                var_h[2] = S.gvar[ty][tx - 2]; var_h[3] = S.gvar[ty][tx + 2];
+                var_v[0] = S.gvar[ty - 1][tx]; var_v[1] = S.gvar[ty + 1][tx];
+                var_v[2] = S.gvar[ty - 2][tx]; var_v[3] = S.gvar[ty + 2][tx];
+                sd_h[0] = S.gsd[ty][tx - 1]; sd_h[1] = S.gsd[ty][tx + 1];
+                sd_h[2] = S.gsd[ty][tx - 2]; sd_h[3] = S.gsd[ty][tx + 2];
+                sd_v[0] = S.gsd[ty - 1][tx]; sd_v[1] = S.gsd[ty + 1][tx];
+                sd_v[2] = S.gsd[ty - 2][tx]; sd_v[3] = S.gsd[ty + 2][tx];
+                mirror(var_h, x, w, vc);
+                mirror(var_v, y, h, vc);
+                mirror(sd_h, x, w, sdc);
+                mirror(sd_v, y, h, sdc);
+            } else {
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                var_h[i] = variance(hh[i], bs, nz);
-                var_v[i] = variance(vv[i], bs, nz);
+                for (int i = 0; i < 4; i++) {
+                    var_h[i] = variance(hh[i], bs, nz);
+                    var_v[i] = variance(vv[i], bs, nz);
+                    sd_h[i] = rt(var_h[i]);
+                    sd_v[i] = rt(var_v[i]);
+                }
+                sdc = rt(variance(c, bs, nz));
             }
             const float sums0 = add(hh[0], hh[1]), sums1 = add(vv[0], vv[1]);
             const float sums2 = add(hh[2], hh[3]), sums3 = add(vv[2], vv[3]);
             float ratio0 = 0.0f, ratio1 = 0.0f;
-            if (c > rt(variance(c, bs, nz))) {
+            if (c > sdc) {
                 const float t0 = add(mul(c, 2.0f), sums2), t1 = add(mul(c, 2.0f), sums3);
                 const float t2 = add(mul(c, -2.0f), sums2), t3 = add(mul(c, -2.0f), sums3);
 #pragma unroll
                 for (int dir = 0; dir < 2; dir++) {
                     const float* dd = dir == 0 ? hh : vv;
-                    const float* vd = dir == 0 ? var_h : var_v;
-                    float sd[4];
-#pragma unroll
-                    for (int i = 0; i < 4; i++) sd[i] = rt(vd[i]);
+                    const float* sd = dir == 0 ? sd_h : sd_v;
                     const float a = sub(dd[0], dd[1]);
                     const float b = sub(dd[2], dd[3]);
                     const bool any = mul(a, b) > 0.0f || mul(sub(dd[2], c), sub(dd[3], c)) > 0.0f ||
@@ -252,10 +322,7 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
                     const float vu = S.vx[uy][ux], vvv = S.vx[vy][vx_];
                     const float su = S.sx[uy][ux], sv = S.sx[vy][vx_];
                     const float tu = S.sg[uy][ux], tv = S.sg[vy][vx_];
-                    const float xx[4] = {xu, xv, xu, xv}, gg[4] = {gu, gv, gu, gv};
-                    const float vx4[4] = {vu, vvv, vu, vvv}, sx4[4] = {su, sv, su, sv};
-                    const float sg4[4] = {tu, tv, tu, tv};
-                    return estimate(xx, gg, vx4, sx4, sg4, g, cs);
+                    return estimate2(xu, xv, gu, gv, vu, vvv, su, sv, tu, tv, g, cs);
                 };
                 const float eh = pair(gy, gxm, gy, gxp);
                 const float ev = pair(gym, gx, gyp, gx);
@@ -350,7 +417,10 @@ cudaError_t launch_linearize(const uint16_t* codes, uint32_t stride, int w, int 
 cudaError_t launch_develop(const DevelopDesc& d, cudaStream_t s) {
     if (d.w <= 0 || d.h <= 0) return cudaSuccess;
     dim3 grid((d.w + TW - 1) / TW, (d.h + TH - 1) / TH);
-    k_develop<<<grid, kDevThreads, 0, s>>>(d);
+    if (d.w >= 4 && d.h >= 4)
+        k_develop<true><<<grid, kDevThreads, 0, s>>>(d);
+    else
+        k_develop<false><<<grid, kDevThreads, 0, s>>>(d);
     count_launch();
     return cudaGetLastError();
 }
