@@ -218,6 +218,63 @@ int prr_decode_noalloc(int device, void* cuda_stream, const prr_frame_info* info
                        const uint8_t* dev_packet, int idct, uint16_t* dev_samples,
                        prr_dev_status* dev_status, uint32_t* dev_skipped);
 
+/* --- batched decode ----------------------------------------------------------- */
+/* Many frames at once -- any mix of sizes, bitstream versions, Bayer
+ * patterns, qscales and tile alignments, at full resolution or reduced --
+ * decoded by one persistent kernel that drains a device queue of work items
+ * from all frames (after one tile-offset pass per frame). No counterpart in
+ * the crate: each job is decode_frame_with (src/decoder.rs:226-267) or
+ * decode_frame_reduced_with (src/reduced.rs:147-201) with the same output,
+ * skipped-tile list and errors. */
+#define PRR_SCALE_FULL 0
+typedef struct prr_job {
+    const uint8_t* packet;   /* host memory; read during prr_batch_submit */
+    uint64_t len;
+    int32_t scale;           /* PRR_SCALE_FULL or a prr_scale */
+    int32_t idct;            /* full resolution: a prr_idct */
+    int32_t greens;          /* reduced: a prr_greens */
+    int32_t status;          /* result: PRR_OK or this frame's error */
+    uint16_t* dev_out;       /* device: coded_width * coded_height u16 (full) or
+                                3 * (coded_width >> s) * (coded_height >> s) u16 (reduced) */
+    uint64_t out_len;
+    prr_decode_result result; /* header, max_qscale, skipped tiles (caller array) */
+    prr_error error;
+} prr_job;
+
+/* Launch shape of the batch kernel, per bucket of batches. */
+typedef struct prr_batch_config {
+    uint32_t ctas_per_sm;  /* persistent CTAs per SM; 0: as many as fit */
+    uint32_t stage_bytes;  /* packet bytes a 64-tile chunk stages in shared memory:
+                              a multiple of 16, at most 98304 */
+    uint32_t use_graph;    /* replay a CUDA graph captured for the bucket */
+    uint32_t pad;
+} prr_batch_config;
+
+/* Parse the jobs' packets, upload them and enqueue the batch on the
+ * context's stream. Jobs whose packet fails to parse or whose arguments are
+ * wrong get their status now and are left out; the others are decoded.
+ * Returns an error only for the call itself (bad context, CUDA failure).
+ * `jobs` must stay valid until prr_batch_wait returns. */
+int prr_batch_submit(prr_ctx* ctx, prr_job* jobs, size_t n);
+/* Wait for the submitted batch (timeout_ms 0: no limit; PRR_ERR_TIMEOUT if
+ * it has not finished, and the batch stays pending) and fill each job's
+ * status, result and error. */
+int prr_batch_wait(prr_ctx* ctx, uint32_t timeout_ms);
+/* Device time of the last batch's kernels, in milliseconds. */
+int prr_batch_last_ms(prr_ctx* ctx, float* ms);
+/* The shape bucket of a batch: ceil(log2) of its frame count and of its
+ * tile count. */
+int prr_batch_bucket(prr_ctx* ctx, const prr_job* jobs, size_t n, uint32_t* bucket);
+/* The autotuner: decodes the batch `reps` times under each candidate launch
+ * shape (stage bytes x CTAs per SM), keeps the fastest as the config of the
+ * batch's bucket and returns it with its median device time. The jobs'
+ * results are those of the last run. */
+int prr_batch_tune(prr_ctx* ctx, prr_job* jobs, size_t n, uint32_t reps, prr_batch_config* best,
+                   float* best_ms);
+/* Set or read the config of a bucket (unset buckets use the default). */
+int prr_batch_set_config(prr_ctx* ctx, uint32_t bucket, const prr_batch_config* cfg);
+int prr_batch_get_config(prr_ctx* ctx, uint32_t bucket, prr_batch_config* cfg);
+
 /* --- linearize ---------------------------------------------------------------- */
 /* Frame::linearize_into, src/decoder.rs:197-216: coded code values (device)
  * -> width*height linear values (device). Asynchronous. */

@@ -599,11 +599,153 @@ def develop_planar_into(frame: Frame, params: DemosaicParams, stage: Stage, out:
     _develop(frame, params, stage, 1, list(out))
 
 
+# ---------------------------------------------------------------------------
+# Batched decode (prr_batch_* in include/prr.h): many frames of any mix of
+# sizes, versions, patterns, qscales and alignments, full or reduced, in one
+# persistent kernel. Each job's result is what decode_frame_with or
+# decode_frame_reduced_with returns for its packet, or the Error it raises.
+
+
+@dataclasses.dataclass
+class BatchJob:
+    packet: object
+    scale: Optional[Scale] = None  # None: full resolution
+    idct: Idct = Idct.APPLE
+    greens: Greens = Greens.FIRST
+
+
+@dataclasses.dataclass
+class BatchConfig:
+    """Launch shape of the batch kernel for one bucket of batches."""
+    ctas_per_sm: int = 0  # 0: as many as fit
+    stage_bytes: int = 32 * 1024
+    use_graph: bool = True
+
+    def _c(self) -> _lib.CBatchConfig:
+        return _lib.CBatchConfig(self.ctas_per_sm, self.stage_bytes, 1 if self.use_graph else 0, 0)
+
+    @staticmethod
+    def _from_c(c: _lib.CBatchConfig) -> "BatchConfig":
+        return BatchConfig(int(c.ctas_per_sm), int(c.stage_bytes), bool(c.use_graph))
+
+
+class BatchDecoder:
+    """A context's batch decoder: submit / wait, per-bucket launch shapes
+    and the autotuner that picks them."""
+
+    def __init__(self, device: Optional[int] = None):
+        self.ctx = context(device)
+
+    def _prepare(self, jobs: Sequence[BatchJob], outs=None):
+        torch = _torch()
+        n = len(jobs)
+        arr = (_lib.CJob * max(1, n))()
+        keep = []
+        frames = []
+        for i, job in enumerate(jobs):
+            buf, ln = _pkt(job.packet)
+            keep.append(buf)
+            cj = arr[i]
+            cj.packet = _ptr(buf)
+            cj.len = ln
+            cj.scale = _lib.SCALE_FULL if job.scale is None else int(job.scale)
+            cj.idct = int(job.idct)
+            cj.greens = int(job.greens)
+            out = None if outs is None else outs[i]
+            ntiles = 1
+            if out is None:
+                try:
+                    info = frame_info(job.packet)
+                    ntiles = max(1, info.ntiles)
+                    cw, ch = info.coded_width, info.coded_height
+                    if job.scale is None:
+                        n_out = cw * ch
+                    else:
+                        n_out = 3 * (cw >> int(job.scale)) * (ch >> int(job.scale))
+                    out = torch.empty(max(1, n_out), dtype=torch.uint16, device="cuda")
+                except Error:
+                    out = torch.empty(1, dtype=torch.uint16, device="cuda")
+            else:
+                try:
+                    ntiles = max(1, frame_info(job.packet).ntiles)
+                except Error:
+                    pass
+            cj.dev_out = _dptr(out)
+            cj.out_len = _numel(out)
+            skipped = (C.c_uint64 * ntiles)()
+            cj.result.skipped = skipped
+            cj.result.skipped_cap = ntiles
+            keep.append(skipped)
+            frames.append((out, skipped))
+        return arr, keep, frames
+
+    def _results(self, jobs, arr, frames) -> List[object]:
+        results = []
+        for i, job in enumerate(jobs):
+            cj = arr[i]
+            if cj.status:
+                results.append(_error(cj.status, cj.error, self.ctx))
+                continue
+            out, skipped = frames[i]
+            header = FrameHeader._from_c(cj.result.header)
+            sk = [int(skipped[k]) for k in range(min(int(cj.result.n_skipped), int(cj.result.skipped_cap)))]
+            if job.scale is None:
+                results.append(Frame(header, out, sk, int(cj.result.max_qscale)))
+            else:
+                results.append(RgbFrame(header, job.scale, job.greens, out, sk, int(cj.result.max_qscale)))
+        return results
+
+    def decode(self, jobs: Sequence[BatchJob], outs=None) -> List[object]:
+        """Decode every job; each result is a Frame, an RgbFrame or an Error.
+        `outs` optionally gives each job's device output tensor."""
+        arr, keep, frames = self._prepare(jobs, outs)
+        L = _lib.lib()
+        _check(L.prr_batch_submit(self.ctx, arr, len(jobs)), ctx=self.ctx)
+        _check(L.prr_batch_wait(self.ctx, 0), ctx=self.ctx)
+        del keep
+        return self._results(jobs, arr, frames)
+
+    def last_ms(self) -> float:
+        """Device time of the last batch's kernels, in milliseconds."""
+        ms = C.c_float()
+        _check(_lib.lib().prr_batch_last_ms(self.ctx, C.byref(ms)), ctx=self.ctx)
+        return float(ms.value)
+
+    def bucket(self, jobs: Sequence[BatchJob]) -> int:
+        arr, keep, _ = self._prepare(jobs)
+        b = C.c_uint32()
+        _check(_lib.lib().prr_batch_bucket(self.ctx, arr, len(jobs), C.byref(b)), ctx=self.ctx)
+        return int(b.value)
+
+    def tune(self, jobs: Sequence[BatchJob], reps: int = 3) -> Tuple[BatchConfig, float]:
+        """Time each candidate launch shape on this batch; the fastest
+        becomes its bucket's config. Returns (config, median ms)."""
+        arr, keep, frames = self._prepare(jobs)
+        best, ms = _lib.CBatchConfig(), C.c_float()
+        _check(_lib.lib().prr_batch_tune(self.ctx, arr, len(jobs), reps, C.byref(best), C.byref(ms)),
+               ctx=self.ctx)
+        return BatchConfig._from_c(best), float(ms.value)
+
+    def set_config(self, bucket: int, cfg: BatchConfig) -> None:
+        c = cfg._c()
+        _check(_lib.lib().prr_batch_set_config(self.ctx, bucket, C.byref(c)), ctx=self.ctx)
+
+    def get_config(self, bucket: int) -> BatchConfig:
+        c = _lib.CBatchConfig()
+        _check(_lib.lib().prr_batch_get_config(self.ctx, bucket, C.byref(c)), ctx=self.ctx)
+        return BatchConfig._from_c(c)
+
+
+def decode_batch(jobs: Sequence[BatchJob]) -> List[object]:
+    """Decode a batch of frames on the current device (see BatchDecoder)."""
+    return BatchDecoder().decode(jobs)
+
+
 __all__ = [
     "BLACK_LEVEL", "PREFIX_LEN", "FOURCCS", "is_prores_raw_fourcc", "Idct", "Scale", "Greens", "Stage",
     "Exposure", "BayerPattern", "Error", "Curve", "FrameHeader", "ParsedFrame", "header_len", "parse_header",
     "parse_frame", "frame_info", "frame_quantizer", "context", "kernel_launches", "Frame", "decode_frame",
     "decode_frame_with", "RgbFrame", "decode_frame_reduced", "decode_frame_reduced_with", "DemosaicParams",
     "output_matrix", "RgbImage", "RgbPlanes", "develop", "develop_with", "develop_into", "develop_planar",
-    "develop_planar_into",
+    "develop_planar_into", "BatchJob", "BatchConfig", "BatchDecoder", "decode_batch",
 ]

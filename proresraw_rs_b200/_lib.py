@@ -117,6 +117,32 @@ class CDevStatus(C.Structure):
     ]
 
 
+class CJob(C.Structure):
+    _fields_ = [
+        ("packet", C.c_void_p),
+        ("len", C.c_uint64),
+        ("scale", C.c_int32),
+        ("idct", C.c_int32),
+        ("greens", C.c_int32),
+        ("status", C.c_int32),
+        ("dev_out", C.c_void_p),
+        ("out_len", C.c_uint64),
+        ("result", CDecodeResult),
+        ("error", CError),
+    ]
+
+
+class CBatchConfig(C.Structure):
+    _fields_ = [
+        ("ctas_per_sm", C.c_uint32),
+        ("stage_bytes", C.c_uint32),
+        ("use_graph", C.c_uint32),
+        ("pad", C.c_uint32),
+    ]
+
+
+SCALE_FULL = 0
+
 _lib = None
 
 
@@ -167,6 +193,13 @@ def lib():
         "prr_transform_blocks": (i, [vp, i, vp, vp, vp, sz]),
         "prr_decode_components": (i, [vp, vp, vp, vp, sz, i, i, vp]),
         "prr_decode_noalloc": (i, [i, vp, P(CFrameInfo), vp, i, vp, vp, vp]),
+        "prr_batch_submit": (i, [vp, P(CJob), sz]),
+        "prr_batch_wait": (i, [vp, C.c_uint32]),
+        "prr_batch_last_ms": (i, [vp, P(C.c_float)]),
+        "prr_batch_bucket": (i, [vp, P(CJob), sz, P(C.c_uint32)]),
+        "prr_batch_tune": (i, [vp, P(CJob), sz, C.c_uint32, P(CBatchConfig), P(C.c_float)]),
+        "prr_batch_set_config": (i, [vp, C.c_uint32, P(CBatchConfig)]),
+        "prr_batch_get_config": (i, [vp, C.c_uint32, P(CBatchConfig)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

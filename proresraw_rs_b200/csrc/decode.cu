@@ -17,6 +17,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstddef>
+
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -70,8 +73,8 @@ __device__ __forceinline__ void tile_geom(uint32_t j, uint32_t columns, uint32_t
 }  // namespace
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_tile_index(FrameDesc d, uint32_t* __restrict__ tile_off,
-                                                     prr_dev_status* __restrict__ st) {
+__device__ __forceinline__ void tile_index_body(const FrameDesc& d, uint32_t* __restrict__ tile_off,
+                                                prr_dev_status* __restrict__ st) {
     __shared__ uint64_t warp_tot[32];
     __shared__ uint32_t red_max[32], red_min[32];
     const uint32_t T = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -131,6 +134,11 @@ __global__ void __launch_bounds__(1024) k_tile_index(FrameDesc d, uint32_t* __re
     }
 }
 
+__global__ void __launch_bounds__(1024) k_tile_index(FrameDesc d, uint32_t* __restrict__ tile_off,
+                                                     prr_dev_status* __restrict__ st) {
+    tile_index_body(d, tile_off, st);
+}
+
 // ---------------------------------------------------------------------------
 // Segment decode, shared by the full and reduced kernels.
 
@@ -154,6 +162,7 @@ struct SegShared {
     uint32_t ntiles;
     uint32_t first_j;  // index within the tile row of the segment's first tile
     uint32_t sq0;      // first 16-sensel column of the segment
+    uint32_t c0[8], cd[8];  // linearization curve (reduced decode)
     __align__(16) int16_t coef[64 * kCoefStride];  // [square * 4 + stream][72]
     __align__(16) uint32_t rowbuf[64 * kRowStride];  // row-pass output, f32 or int32 bits
 };
@@ -167,14 +176,19 @@ __device__ __forceinline__ uint32_t stream_list_base(const FrameDesc& d, uint32_
 }
 
 // Parse this segment's tiles and zero the coefficient buffer; returns the
-// number of 16-sensel columns (squares) of the segment.
+// number of 16-sensel columns (squares) of the segment. A CTA that keeps
+// its code tables across segments passes load_code_tables = false.
 __device__ __forceinline__ uint32_t seg_setup(SegShared& S, const FrameDesc& d,
                                               const uint32_t* __restrict__ tile_off,
                                               prr_dev_status* st, uint32_t* skipped,
-                                              uint32_t seg, uint32_t trow) {
+                                              uint32_t seg, uint32_t trow, bool load_code_tables = true) {
     const uint32_t tid = threadIdx.x;
-    load_tables(&S.T);
+    if (load_code_tables) load_tables(&S.T);
     if (tid < 16) reinterpret_cast<uint32_t*>(S.qmat)[tid] = reinterpret_cast<const uint32_t*>(d.qmat)[tid];
+    if (tid < 8) {
+        S.c0[tid] = d.curve_c0[tid];
+        S.cd[tid] = d.curve_delta[tid];
+    }
     {
         uint4* c = reinterpret_cast<uint4*>(S.coef);
         for (uint32_t i = tid; i < 64 * kCoefStride * 2 / 16; i += kThreads) c[i] = make_uint4(0, 0, 0, 0);
@@ -266,7 +280,9 @@ __device__ __forceinline__ void seg_decode_stream(SegShared& S, const FrameDesc&
 // one warp per stream, lanes over the list's (position, value) entries.
 // A stream whose zero run wrapped back over stored positions may hold a
 // position twice; it is replayed in order by one lane so the later value
-// wins, as on the host.
+// wins, as on the host. COHERENT reads the counts and lists through L2 only,
+// for lists another CTA wrote during the same launch.
+template <bool COHERENT = false>
 __device__ __forceinline__ void seg_scatter(SegShared& S, const FrameDesc& d, uint32_t trow,
                                             uint32_t log2_coefs, bool second_green, prr_dev_status* st) {
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -277,7 +293,7 @@ __device__ __forceinline__ void seg_scatter(SegShared& S, const FrameDesc& d, ui
         const SegTile& tl = S.tiles[t];
         if (!tl.valid || (s == 1 && !second_green)) continue;
         const uint32_t g = (first_tile + t) * 4 + s;
-        const uint32_t cnt = d.counts[g];
+        const uint32_t cnt = COHERENT ? __ldcg(d.counts + g) : d.counts[g];
         const uint32_t n = cnt & 0x7FFFFFFFu;
         const uint32_t* list = d.pairs + stream_list_base(d, trow, tl.x_rel + S.sq0, tl.log2, s, lc);
         int16_t* base = S.coef + (tl.x_rel * 4 + s) * kCoefStride;
@@ -299,22 +315,22 @@ __device__ __forceinline__ void seg_scatter(SegShared& S, const FrameDesc& d, ui
             // holds): decode the stream again here, in order.
             if (lane == 0) seg_decode_stream(S, d, t, s, lc, st);
         } else {
-            for (uint32_t i = lane; i < n; i += 32) put(__ldg(list + i));
+            for (uint32_t i = lane; i < n; i += 32) put(COHERENT ? __ldcg(list + i) : __ldg(list + i));
         }
     }
 }
 
-template <int IDCT, bool SPLIT>
-__global__ void __launch_bounds__(kThreads) k_decode_full(FrameDesc d, const uint32_t* __restrict__ tile_off,
-                                                         prr_dev_status* __restrict__ st,
-                                                         uint32_t* __restrict__ skipped,
-                                                         uint16_t* __restrict__ out) {
-    __shared__ SegShared S;
+// Full-resolution decode of segment `seg` of tile row `trow` (the CTA's
+// work in k_decode_full and the batch kernel). PERSIST: the CTA keeps its
+// code tables and the lists come from the same launch.
+template <int IDCT, bool SPLIT, bool PERSIST>
+__device__ __forceinline__ void full_segment(SegShared& S, const FrameDesc& d, uint32_t seg, uint32_t trow,
+                                             const uint32_t* __restrict__ tile_off, prr_dev_status* st,
+                                             uint32_t* skipped, uint16_t* __restrict__ out) {
     const uint32_t tid = threadIdx.x;
-    const uint32_t seg = blockIdx.x, trow = blockIdx.y;
-    const uint32_t nsq = seg_setup(S, d, tile_off, st, skipped, seg, trow);
+    const uint32_t nsq = seg_setup(S, d, tile_off, st, skipped, seg, trow, !PERSIST);
     if (SPLIT) {
-        seg_scatter(S, d, trow, 6, true, st);
+        seg_scatter<PERSIST>(S, d, trow, 6, true, st);
     } else {
         // Entropy decoding in the CTA: one thread per component stream.
         if (tid < 4 * S.ntiles) seg_decode_stream(S, d, tid >> 2, tid & 3, 6, st);
@@ -393,28 +409,31 @@ __global__ void __launch_bounds__(kThreads) k_decode_full(FrameDesc d, const uin
     }
 }
 
+template <int IDCT, bool SPLIT>
+__global__ void __launch_bounds__(kThreads) k_decode_full(FrameDesc d, const uint32_t* __restrict__ tile_off,
+                                                         prr_dev_status* __restrict__ st,
+                                                         uint32_t* __restrict__ skipped,
+                                                         uint16_t* __restrict__ out) {
+    __shared__ SegShared S;
+    full_segment<IDCT, SPLIT, false>(S, d, blockIdx.x, blockIdx.y, tile_off, st, skipped, out);
+}
+
 // Reduced-resolution decode (src/reduced.rs:217-273): red from stream 3,
 // green from stream 0 (averaged with stream 1 for Greens::Average), blue
 // from stream 2, through the 8x8, 4x4 or 2x2 transform and the curve.
-template <int SHIFT, bool SPLIT>
-__global__ void __launch_bounds__(kThreads) k_decode_reduced(FrameDesc d, int greens,
-                                                            const uint32_t* __restrict__ tile_off,
-                                                            prr_dev_status* __restrict__ st,
-                                                            uint32_t* __restrict__ skipped,
-                                                            uint16_t* __restrict__ out) {
-    __shared__ SegShared S;
-    __shared__ uint32_t c0[8], cd[8];
+template <int SHIFT, bool SPLIT, bool PERSIST>
+__device__ __forceinline__ void reduced_segment(SegShared& S, const FrameDesc& d, int greens, uint32_t seg,
+                                                uint32_t trow, const uint32_t* __restrict__ tile_off,
+                                                prr_dev_status* st, uint32_t* skipped,
+                                                uint16_t* __restrict__ out) {
     constexpr uint32_t LC = SHIFT == 1 ? 6 : (SHIFT == 2 ? 4 : 2);
     constexpr uint32_t SIDE = 16 >> SHIFT;  // output pixels per square side
     const uint32_t tid = threadIdx.x;
-    const uint32_t seg = blockIdx.x, trow = blockIdx.y;
-    if (tid < 8) {
-        c0[tid] = d.curve_c0[tid];
-        cd[tid] = d.curve_delta[tid];
-    }
-    const uint32_t nsq = seg_setup(S, d, tile_off, st, skipped, seg, trow);
+    const uint32_t* c0 = S.c0;
+    const uint32_t* cd = S.cd;
+    const uint32_t nsq = seg_setup(S, d, tile_off, st, skipped, seg, trow, !PERSIST);
     if (SPLIT) {
-        seg_scatter(S, d, trow, LC, greens != 0, st);
+        seg_scatter<PERSIST>(S, d, trow, LC, greens != 0, st);
     } else {
         const uint32_t s = tid & 3;
         if (tid < 4 * S.ntiles && (s != 1 || greens)) seg_decode_stream(S, d, tid >> 2, s, LC, st);
@@ -509,6 +528,16 @@ __global__ void __launch_bounds__(kThreads) k_decode_reduced(FrameDesc d, int gr
         dst[1] = rgb[1];
         dst[2] = rgb[2];
     }
+}
+
+template <int SHIFT, bool SPLIT>
+__global__ void __launch_bounds__(kThreads) k_decode_reduced(FrameDesc d, int greens,
+                                                            const uint32_t* __restrict__ tile_off,
+                                                            prr_dev_status* __restrict__ st,
+                                                            uint32_t* __restrict__ skipped,
+                                                            uint16_t* __restrict__ out) {
+    __shared__ SegShared S;
+    reduced_segment<SHIFT, SPLIT, false>(S, d, greens, blockIdx.x, blockIdx.y, tile_off, st, skipped, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -656,7 +685,7 @@ __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off,
                                                    bool& revisited, bool& ok) {
     const uint32_t blocks = 1u << log2_blocks;
     const uint32_t codes = blocks << LC;
-    Reader<Src> r;
+    LeanReader<Src> r;
     r.init(src, off, len);
     uint32_t cnt = 0, e0 = 0, e1 = 0, e2 = 0, e3 = 0;
     // Append the coefficient at interleaved position n (DCs are 0..blocks-1).
@@ -749,29 +778,29 @@ __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off,
 // on average. Larger spans are read from global memory instead.
 constexpr uint32_t kStageBytes = 32 * 1024;
 
+// Entropy-decode the streams of tiles [chunk * blockDim.x / 4, ...) of a
+// frame, one stream per thread. `stage` holds stage_bytes + 16 bytes of
+// shared memory; the chunk's packet span is copied there when it fits.
+// Ends with the CTA's threads at different points (no barrier).
 template <uint32_t LC>
-__global__ void __launch_bounds__(128) k_entropy(FrameDesc d, int greens, const uint32_t* __restrict__ tile_off,
-                                                 prr_dev_status* __restrict__ st) {
-    __shared__ CodeTables CT;
-    __shared__ EntropyTables T;
-    __shared__ __align__(16) uint32_t stage[kStageBytes / 4 + 4];  // + the word after the last byte
-    load_tables(&CT);
-    __syncthreads();
-    build_entropy_tables(T, CT);
-    // The CTA's tiles [t0, t1) occupy bytes [tile_off[t0], tile_off[t1]).
-    const uint32_t t0 = blockIdx.x * (blockDim.x / 4);
+__device__ __forceinline__ void entropy_chunk(const EntropyTables& T, uint32_t* stage, uint32_t stage_bytes,
+                                              const FrameDesc& d, int greens,
+                                              const uint32_t* __restrict__ tile_off, prr_dev_status* st,
+                                              uint32_t chunk) {
+    // The chunk's tiles [t0, t1) occupy bytes [tile_off[t0], tile_off[t1]).
+    const uint32_t t0 = chunk * (blockDim.x / 4);
     const uint32_t t1 = min(t0 + blockDim.x / 4, d.ntiles);
     const uint32_t hi = min(tile_off[t1], d.len);
     const uint32_t lo = min(tile_off[t0], hi);
     const uint32_t base = lo & ~15u, top = (hi + 15) & ~15u;  // within the padded packet buffer
-    const bool staged = top - base <= kStageBytes;
+    const bool staged = top - base <= stage_bytes;
     if (staged) {
         const uint4* src = reinterpret_cast<const uint4*>(d.words) + base / 16;
         uint4* dst = reinterpret_cast<uint4*>(stage);
         for (uint32_t i = threadIdx.x; i < (top - base) / 16; i += blockDim.x) dst[i] = __ldg(src + i);
     }
     __syncthreads();
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t g = chunk * blockDim.x + threadIdx.x;
     if (g >= 4 * d.ntiles) return;
     const uint32_t tile = g >> 2, s = g & 3;
     if (LC != 6 && s == 1 && !greens) return;  // a reduced decode reads the second green only to average
@@ -795,6 +824,18 @@ __global__ void __launch_bounds__(128) k_entropy(FrameDesc d, int greens, const 
                : entropy_events<LC>(GlobalWords{d.words}, soff, slen, log2, T, list, revisited, ok);
     if (!ok) atomicOr(&st->error, 1u);
     d.counts[g] = revisited ? 0x80000000u : cnt;
+}
+
+template <uint32_t LC>
+__global__ void __launch_bounds__(128) k_entropy(FrameDesc d, int greens, const uint32_t* __restrict__ tile_off,
+                                                 prr_dev_status* __restrict__ st) {
+    __shared__ CodeTables CT;
+    __shared__ EntropyTables T;
+    __shared__ __align__(16) uint32_t stage[kStageBytes / 4 + 4];  // + the word after the last byte
+    load_tables(&CT);
+    __syncthreads();
+    build_entropy_tables(T, CT);
+    entropy_chunk<LC>(T, stage, kStageBytes, d, greens, tile_off, st, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -866,6 +907,204 @@ __global__ void k_decode_components(const uint32_t* __restrict__ words, const ui
     bool revisited = false;
     decode_component(GlobalWords{words}, off[i], len[i], uint32_t(log2_blocks), uint32_t(log2_coefs), T,
                      [&](uint32_t idx, int16_t v) { dst[idx] = v; }, revisited);
+}
+
+// ---------------------------------------------------------------------------
+// Batch decode: one CTA per frame for the tile offsets, then one persistent
+// launch for the entropy chunks and transform segments of all frames.
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait until *flag == want, for at most ~limit_ns (and a fixed number of
+// polls); false when the limit ran out.
+__device__ __forceinline__ bool wait_flag(const uint32_t* flag, uint32_t want, uint64_t limit_ns) {
+    if (ld_acquire_gpu(flag) == want) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0; it < (1u << 26); it++) {
+        __nanosleep(128);
+        if (ld_acquire_gpu(flag) == want) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+    return false;
+}
+
+constexpr uint64_t kChunkWaitNs = 2000000000ull;  // 2 s
+
+__global__ void __launch_bounds__(1024) k_batch_tile_index(BatchDesc b) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        b.q->head = 0;
+        b.q->error = 0;
+        b.q->epoch = b.q->epoch + 1;
+    }
+    if (blockIdx.x >= b.hdr->nframes) return;
+    const BatchFrame& F = b.frames[blockIdx.x];
+    tile_index_body(F.d, F.tile_off, F.st);
+}
+
+// Last frame whose first item of the kind is <= key (frames without items
+// of the kind share their successor's first item and are passed over).
+__device__ __forceinline__ uint32_t batch_frame_of(const BatchDesc& b, uint32_t nframes, uint32_t key,
+                                                  bool entropy) {
+    uint32_t lo = 0, hi = nframes;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t begin = entropy ? b.frames[mid].ent_begin : b.frames[mid].seg_begin;
+        if (begin <= key)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// The batch kernel's work items as separate functions, so that each gets
+// the registers it needs on its own instead of the sum of all of them.
+template <uint32_t LC>
+__device__ __noinline__ void batch_entropy(const EntropyTables& T, uint32_t* stage, uint32_t stage_bytes,
+                                           const FrameDesc& d, int greens, const uint32_t* tile_off,
+                                           prr_dev_status* st, uint32_t chunk) {
+    entropy_chunk<LC>(T, stage, stage_bytes, d, greens, tile_off, st, chunk);
+}
+template <int IDCT>
+__device__ __noinline__ void batch_full(SegShared& S, const FrameDesc& d, uint32_t seg, uint32_t trow,
+                                        const uint32_t* tile_off, prr_dev_status* st, uint32_t* skipped,
+                                        uint16_t* out) {
+    full_segment<IDCT, true, true>(S, d, seg, trow, tile_off, st, skipped, out);
+}
+template <int SHIFT>
+__device__ __noinline__ void batch_reduced(SegShared& S, const FrameDesc& d, int greens, uint32_t seg,
+                                           uint32_t trow, const uint32_t* tile_off, prr_dev_status* st,
+                                           uint32_t* skipped, uint16_t* out) {
+    reduced_segment<SHIFT, true, true>(S, d, greens, seg, trow, tile_off, st, skipped, out);
+}
+
+// The work items are claimed in order, so every chunk has been claimed by a
+// running CTA before any segment is: the waits of a segment always end,
+// whatever the grid size. The code tables and the codeword table are built
+// once per CTA. The packet stage of a chunk aliases the segment buffers.
+__global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    SegShared& S = *reinterpret_cast<SegShared*>(dyn_smem);
+    uint32_t* stage = reinterpret_cast<uint32_t*>(S.coef);
+    __shared__ EntropyTables T;
+    __shared__ FrameDesc fd;
+    __shared__ uint32_t s_item, s_frame, s_epoch, s_ok;
+    const uint32_t tid = threadIdx.x;
+    load_tables(&S.T);
+    if (tid == 0) s_epoch = b.q->epoch;
+    __syncthreads();
+    build_entropy_tables(T, S.T);
+    const uint32_t nframes = b.hdr->nframes, ent_items = b.hdr->ent_items;
+    const uint32_t total = ent_items + b.hdr->seg_items;
+    for (;;) {
+        __syncthreads();  // the previous item's shared memory is no longer read
+        if (tid == 0) {
+            const uint32_t item = atomicAdd(&b.q->head, 1u);
+            s_item = item;
+            if (item < total) {
+                const bool ent = item < ent_items;
+                s_frame = batch_frame_of(b, nframes, ent ? item : item - ent_items, ent);
+            }
+        }
+        __syncthreads();
+        const uint32_t item = s_item;
+        if (item >= total) break;
+        const BatchFrame& F = b.frames[s_frame];
+        for (uint32_t i = tid; i < sizeof(FrameDesc) / 4; i += kBatchThreads)
+            reinterpret_cast<uint32_t*>(&fd)[i] = reinterpret_cast<const uint32_t*>(&F.d)[i];
+        const uint32_t shift = F.shift, lc = F.lc, greens = F.greens;
+        if (item < ent_items) {
+            __syncthreads();
+            const uint32_t chunk = item - F.ent_begin;
+            if (lc == 6)
+                batch_entropy<6>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk);
+            else if (lc == 4)
+                batch_entropy<4>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk);
+            else
+                batch_entropy<2>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk);
+            __syncthreads();
+            if (tid == 0) {
+                __threadfence();
+                st_release_gpu(b.flags + item, s_epoch);
+            }
+            continue;
+        }
+        const uint32_t local = item - ent_items - F.seg_begin;
+        const uint32_t trow = local / F.d.segs_per_row, seg = local - trow * F.d.segs_per_row;
+        if (tid == 0) {
+            // The segment's tiles lie among the 16 tiles of the row from its
+            // first one (seg_setup's j0); wait for the chunks holding them.
+            const uint32_t a = F.d.alignment, cols = F.d.columns, sq0 = seg * 16;
+            const uint32_t fullsq = (cols >> a) << a;
+            const uint32_t j0 = sq0 < fullsq ? (sq0 >> a) : (cols >> a);
+            const uint32_t first = trow * F.d.tiles_per_row + j0;
+            const uint32_t last = trow * F.d.tiles_per_row + min(j0 + 15, F.d.tiles_per_row - 1);
+            bool ok = true;
+            for (uint32_t c = first / kBatchTilesPerChunk; ok && c <= last / kBatchTilesPerChunk; c++)
+                ok = wait_flag(b.flags + F.ent_begin + c, s_epoch, kChunkWaitNs);
+            if (!ok) {
+                atomicOr(&b.q->error, 1u);
+                atomicOr(&F.st->error, 2u);
+            }
+            s_ok = ok ? 1u : 0u;
+        }
+        __syncthreads();
+        if (!s_ok) continue;  // the segment is left unwritten; the frame reports the timeout
+        if (shift == 0) {
+            if (F.idct == PRR_IDCT_FFMPEG)
+                batch_full<PRR_IDCT_FFMPEG>(S, fd, seg, trow, F.tile_off, F.st, F.skipped, F.out);
+            else
+                batch_full<PRR_IDCT_APPLE>(S, fd, seg, trow, F.tile_off, F.st, F.skipped, F.out);
+        } else if (shift == 1) {
+            batch_reduced<1>(S, fd, int(greens), seg, trow, F.tile_off, F.st, F.skipped, F.out);
+        } else if (shift == 2) {
+            batch_reduced<2>(S, fd, int(greens), seg, trow, F.tile_off, F.st, F.skipped, F.out);
+        } else {
+            batch_reduced<3>(S, fd, int(greens), seg, trow, F.tile_off, F.st, F.skipped, F.out);
+        }
+    }
+}
+
+size_t batch_smem_bytes(uint32_t stage_bytes) {
+    const size_t stage_end = offsetof(SegShared, coef) + size_t(stage_bytes) + 16;
+    return std::max(sizeof(SegShared), (stage_end + 15) & ~size_t(15));
+}
+
+// Allow the largest stage on the current device (once per device, before
+// any capture).
+cudaError_t batch_prepare_device() {
+    return cudaFuncSetAttribute(k_batch_decode, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(batch_smem_bytes(kBatchMaxStageBytes)));
+}
+
+cudaError_t batch_max_ctas_per_sm(uint32_t stage_bytes, int* ctas) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas, k_batch_decode, kBatchThreads,
+                                                         batch_smem_bytes(stage_bytes));
+}
+
+cudaError_t launch_batch_tile_index(const BatchDesc& b, uint32_t grid, cudaStream_t s) {
+    k_batch_tile_index<<<std::max(grid, 1u), 1024, 0, s>>>(b);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_decode(const BatchDesc& b, uint32_t ctas, cudaStream_t s) {
+    if (b.stage_bytes > kBatchMaxStageBytes || (b.stage_bytes & 15) != 0) return cudaErrorInvalidValue;
+    k_batch_decode<<<std::max(ctas, 1u), kBatchThreads, batch_smem_bytes(b.stage_bytes), s>>>(b);
+    count_launch();
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------

@@ -51,6 +51,61 @@ cudaError_t launch_decode_full(const FrameDesc& d, int idct, const uint32_t* til
 cudaError_t launch_decode_reduced(const FrameDesc& d, int shift, int greens,
                                   const uint32_t* tile_off, prr_dev_status* st, uint32_t* skipped,
                                   uint16_t* out, cudaStream_t s);
+// Batch decode: the frames of a batch in one persistent launch that drains
+// a queue of work items: first the entropy chunks of every frame (a chunk is
+// the streams of threads / 4 consecutive tiles), then the transform
+// segments of every frame (tile row x 256-sensel segment). A segment waits
+// for the chunk flags of its tiles, set to the batch's epoch.
+struct BatchFrame {
+    FrameDesc d;            // counts / pairs point into the batch scratch
+    uint32_t* tile_off;     // ntiles + 1 offsets
+    prr_dev_status* st;
+    uint32_t* skipped;      // ntiles entries
+    uint16_t* out;
+    uint32_t shift;         // 0: full resolution; 1..3: reduced by 2^shift
+    uint32_t idct;          // full resolution
+    uint32_t greens;        // reduced
+    uint32_t lc;            // log2 coefficients decoded per block
+    uint32_t ent_begin;     // first entropy item (chunk) of the frame
+    uint32_t seg_begin;     // first transform item of the frame, counted after all chunks
+    uint32_t pad[2];
+};
+
+struct BatchQueue {
+    uint32_t head;   // next work item
+    uint32_t epoch;  // batch sequence number; chunk flags hold it when done
+    uint32_t error;  // a wait for a chunk ran out of time
+    uint32_t pad;
+};
+
+// Sizes of the current batch, uploaded with its frames, so that one launch
+// (or one captured graph) serves every batch that fits the buffers.
+struct BatchHeader {
+    uint32_t nframes;
+    uint32_t ent_items;  // chunks of all frames
+    uint32_t seg_items;  // segments of all frames
+    uint32_t pad;
+};
+
+struct BatchDesc {
+    const BatchHeader* hdr;
+    const BatchFrame* frames;
+    BatchQueue* q;
+    uint32_t* flags;  // one per chunk
+    uint32_t stage_bytes;
+};
+
+constexpr uint32_t kBatchThreads = 256;
+constexpr uint32_t kBatchTilesPerChunk = kBatchThreads / 4;
+constexpr uint32_t kBatchMaxStageBytes = 96 * 1024;
+// Dynamic shared memory of the batch kernel for a packet stage of
+// stage_bytes (<= kBatchMaxStageBytes), and the CTAs per SM that fit.
+size_t batch_smem_bytes(uint32_t stage_bytes);
+cudaError_t batch_prepare_device();
+cudaError_t batch_max_ctas_per_sm(uint32_t stage_bytes, int* ctas);
+cudaError_t launch_batch_tile_index(const BatchDesc& b, uint32_t grid, cudaStream_t s);
+cudaError_t launch_batch_decode(const BatchDesc& b, uint32_t ctas, cudaStream_t s);
+
 cudaError_t launch_transform_blocks(int kind, const int16_t* coefs, const int16_t* q,
                                     uint16_t* out, size_t n, cudaStream_t s);
 cudaError_t launch_decode_components(const uint8_t* packet, const uint32_t* off,

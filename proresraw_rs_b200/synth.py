@@ -328,3 +328,54 @@ def corrupt_tiles(packet: bytes, fraction: float, seed: int):
     idx = np.empty(min(n_t, 1 << 20), dtype=np.uint64)
     n = lib().prs_corrupt_tiles(buf.ctypes.data, buf.size, fraction, seed, idx.ctypes.data, idx.size)
     return buf.tobytes(), [int(i) for i in idx[:n]]
+
+
+# Sizes of the mixed-batch workload: HD, DCI 4K, 5.8K, 8K.
+BATCH_SIZES = ((1920, 1080), (4096, 2160), (5760, 3040), (8192, 4320))
+
+
+@dataclasses.dataclass
+class BatchItem:
+    """One frame of a mixed batch: its packet and how it is decoded."""
+
+    packet: bytes
+    width: int
+    height: int
+    version: int
+    pattern: int
+    qscale: int
+    alignment: int
+    scale: int   # 0: full resolution, else log2 of the reduction
+    greens: int  # reduced: 0 first green, 1 average
+    corrupt_tiles: Sequence[int] = ()
+
+
+def mixed_batch(n: int, seed: int, sizes=BATCH_SIZES, corrupt: float = 0.0, sigma=(4.0, 32.0),
+                threads: int = 0) -> List[BatchItem]:
+    """A seeded batch of frames of uneven shape: size from `sizes`, bitstream
+    version 0 or 1, RGGB or BGGR, qscale uniform in [15, 45], tile alignment
+    uniform in [0, 4]; half of them decoded at full resolution, half reduced
+    (Half / Quarter / Eighth, first or averaged greens). Mosaics come from
+    mosaic() with sigma uniform in `sigma`; `corrupt` is the fraction of tiles
+    byte-corrupted per frame."""
+    rng = np.random.default_rng(seed)
+    items = []
+    for i in range(n):
+        w, h = sizes[int(rng.integers(len(sizes)))]
+        version = int(rng.integers(2))
+        pattern = (RGGB, BGGR)[int(rng.integers(2))]
+        qscale = int(rng.integers(15, 46))
+        alignment = int(rng.integers(5))
+        scale = 0 if i % 2 == 0 else int(rng.integers(1, 4))
+        greens = int(rng.integers(2)) if scale else 0
+        s = float(rng.uniform(*sigma))
+        mseed = int(rng.integers(1 << 31))
+        m = mosaic(w, h, pattern, seed=mseed, sigma=s, threads=threads)
+        spec = Spec(w, h, pattern=pattern, alignment=alignment, white_level=4095, version=version,
+                    valid_tiles=True)
+        pkt = encode(spec, m, qscale=qscale, qscale_seed=mseed, threads=threads)
+        bad: List[int] = []
+        if corrupt > 0:
+            pkt, bad = corrupt_tiles(pkt, corrupt, seed=mseed)
+        items.append(BatchItem(pkt, w, h, version, pattern, qscale, alignment, scale, greens, bad))
+    return items

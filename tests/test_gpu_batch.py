@@ -1,0 +1,144 @@
+"""The batched decode (prr_batch_*): every job of a mixed batch must give
+what the oracle's decode_frame_with / decode_frame_reduced_with gives for
+its packet -- code values or linear RGB bit-exact, the same skipped tiles and
+max_qscale, or the same error -- whatever the launch shape, with or without
+graph replay, and after the autotuner has run."""
+
+import numpy as np
+import pytest
+
+import _oracle as O
+import proresraw_rs_b200 as P
+from proresraw_rs_b200 import synth as S
+
+pytestmark = pytest.mark.gpu
+
+SMALL_SIZES = ((192, 108), (256, 144), (360, 190), (512, 270), (66, 30))
+
+
+def jobs_of(items, idct=P.Idct.APPLE):
+    return [P.BatchJob(it.packet, None if it.scale == 0 else P.Scale(it.scale), idct, P.Greens(it.greens))
+            for it in items]
+
+
+def oracle_of(job):
+    try:
+        if job.scale is None:
+            return O.decode_frame(bytes(job.packet), int(job.idct))
+        return O.decode_frame_reduced(bytes(job.packet), int(job.scale), int(job.greens))
+    except O.OracleError as e:
+        return e
+
+
+def assert_job(job, got, want):
+    if isinstance(want, O.OracleError):
+        assert isinstance(got, P.Error), got
+        assert got.code == want.code
+        if want.code in (P._lib.ERR_TILE_OUT_OF_BOUNDS,):
+            assert got.fields["tile"] == want.err.index
+        return
+    assert not isinstance(got, P.Error), got
+    host = got.samples_host()
+    assert np.array_equal(host, want.samples)
+    assert got.skipped_tiles == want.skipped_tiles
+    assert got.max_qscale == want.max_qscale
+
+
+def run_and_check(dec, jobs):
+    results = dec.decode(jobs)
+    assert len(results) == len(jobs)
+    for job, got in zip(jobs, results):
+        assert_job(job, got, oracle_of(job))
+    return results
+
+
+@pytest.fixture(scope="module")
+def corpus():
+    return S.mixed_batch(24, seed=2, sizes=SMALL_SIZES, corrupt=0.02)
+
+
+def test_mixed_batch_matches_the_oracle(corpus):
+    dec = P.BatchDecoder()
+    run_and_check(dec, jobs_of(corpus))
+    assert dec.last_ms() > 0
+
+
+def test_mixed_batch_ffmpeg_idct(corpus):
+    run_and_check(P.BatchDecoder(), jobs_of(corpus, P.Idct.FFMPEG))
+
+
+def test_corrupted_frames_keep_their_skipped_lists(corpus):
+    jobs = jobs_of(corpus)
+    results = P.BatchDecoder().decode(jobs)
+    skipped = sum(len(r.skipped_tiles) for r in results)
+    assert skipped > 0
+    for job, got in zip(jobs, results):
+        assert_job(job, got, oracle_of(job))
+
+
+@pytest.mark.parametrize("stage,per_sm,graph", [(16384, 1, True), (32768, 0, False), (65536, 2, True),
+                                                (98304, 1, True)])
+def test_every_launch_shape_gives_the_same_frames(corpus, stage, per_sm, graph):
+    dec = P.BatchDecoder()
+    jobs = jobs_of(corpus)
+    dec.set_config(dec.bucket(jobs), P.BatchConfig(per_sm, stage, graph))
+    run_and_check(dec, jobs)
+
+
+def test_graph_replay_reads_each_new_batch(corpus):
+    # Two batches of one bucket with different contents: the second replay
+    # must decode the second batch, not repeat the first.
+    dec = P.BatchDecoder()
+    a = jobs_of(corpus[:8])
+    b = a[::-1]  # same bucket, another frame table
+    assert dec.bucket(a) == dec.bucket(b)
+    for jobs in (a, b, jobs_of(corpus[8:16]), a):
+        run_and_check(dec, jobs)
+
+
+def test_errors_are_reported_per_job(corpus):
+    good = jobs_of(corpus[:4])
+    pkt = corpus[0].packet
+    truncated = P.BatchJob(pkt[:40])
+    bad_tag = P.BatchJob(pkt[:4] + b"xxxx" + pkt[8:])
+    # A size table entry reaching past the packet: TileOutOfBounds.
+    oob = bytearray(corpus[2].packet)
+    table = P.frame_info(bytes(oob)).table_offset
+    oob[table] = 0xFF
+    oob[table + 1] = 0xFF
+    oob_job = P.BatchJob(bytes(oob), None)
+    jobs = [good[0], truncated, good[1], bad_tag, oob_job, good[2], good[3]]
+    results = P.BatchDecoder().decode(jobs)
+    for job, got in zip(jobs, results):
+        assert_job(job, got, oracle_of(job))
+    assert isinstance(results[1], P.Error) and isinstance(results[3], P.Error)
+
+
+def test_wrong_output_size_is_a_buffer_error(corpus):
+    import torch
+
+    job = jobs_of(corpus[:1])[0]
+    out = torch.empty(7, dtype=torch.uint16, device="cuda")
+    (res,) = P.BatchDecoder().decode([job], outs=[out])
+    assert isinstance(res, P.Error) and res.code == P._lib.ERR_BUFFER
+
+
+def test_empty_and_all_invalid_batches():
+    dec = P.BatchDecoder()
+    assert dec.decode([]) == []
+    res = dec.decode([P.BatchJob(b"\x00" * 12), P.BatchJob(b"")])
+    assert all(isinstance(r, P.Error) for r in res)
+
+
+def test_autotuner_picks_a_config_and_frames_stay_exact(corpus):
+    dec = P.BatchDecoder()
+    jobs = jobs_of(corpus[:12])
+    cfg, ms = dec.tune(jobs, reps=1)
+    assert ms > 0 and cfg.stage_bytes % 16 == 0 and cfg.ctas_per_sm >= 1
+    assert dec.get_config(dec.bucket(jobs)) == cfg
+    run_and_check(dec, jobs)
+
+
+def test_batch_of_one_large_frame_matches_single_decode():
+    items = S.mixed_batch(2, seed=11, sizes=((1920, 1080),), corrupt=0.005)
+    run_and_check(P.BatchDecoder(), jobs_of(items))
