@@ -296,6 +296,61 @@ int prr_develop(prr_ctx* ctx, const prr_header* header, const prr_params* params
                 const uint16_t* dev_samples, int layout, float* r, float* g, float* b,
                 size_t out_len);
 
+/* --- learned develop ---------------------------------------------------------- */
+/* A small convolutional network on the tensor cores (bf16 products, f32
+ * accumulation) offered beside the plain develop: input the half-resolution
+ * Bayer quads (colour differences against the quad's mean green, green level,
+ * gradients and Laplacian) plus a noise channel from the plain develop's
+ * noise model,
+ * six 3x3 conv layers of 32 channels with ReLU, a 3x3 head of 12 channels
+ * shuffled to full-resolution RGB on top of each quad's own colour. No
+ * counterpart in the crate. Parameters are f32, layer by layer (weights
+ * [cout][cin][9], bias [cout]; cin 16 then 32, cout 32 then 16 for the
+ * head), prr_sg_param_count() of them. */
+size_t prr_sg_param_count(void);
+
+typedef struct prr_sg_model {
+    const float* dev_params; /* device, prr_sg_param_count() floats */
+    float noise_lo, noise_hi; /* range of the noise channel the network was trained on */
+} prr_sg_model;
+
+/* develop_into / develop_planar_into (src/demosaic.rs:223-261) by the
+ * network, for the white-balanced and Rec.2020 stages (Demosaiced: white
+ * balance 1). A 32x32 tile in which any quad's noise channel leaves
+ * [noise_lo, noise_hi] is developed by the plain kernel instead (the
+ * per-tile fallback); `fallback_tiles` (nullable; when given the call waits
+ * for the device) receives how many. Buffers as for prr_develop. */
+int prr_develop_learned(prr_ctx* ctx, const prr_header* header, const prr_params* params, int stage,
+                        const uint16_t* dev_samples, const prr_sg_model* model, int layout, float* r,
+                        float* g, float* b, size_t out_len, uint32_t* fallback_tiles);
+
+/* Training on the device with the library's own forward (tensor cores) and
+ * backward (f32) kernels and Adam. Frames are added decoded; their plain
+ * white-balanced develop is the target. A step trains on `batch` crops of
+ * crop x crop pixels (frame index, x, y; x and y even, the crop inside the
+ * frame) with 8 quads of context around each. */
+typedef struct prr_sg_trainer prr_sg_trainer;
+int prr_sg_trainer_create(prr_ctx* ctx, uint32_t batch, uint32_t crop, prr_sg_trainer** out);
+void prr_sg_trainer_destroy(prr_sg_trainer* t);
+int prr_sg_trainer_add_frame(prr_sg_trainer* t, const prr_header* header, const prr_params* params,
+                             const uint16_t* dev_samples, uint32_t* index);
+/* The noise-channel range over the frames added so far. */
+int prr_sg_trainer_noise_range(prr_sg_trainer* t, float* lo, float* hi);
+/* Host parameters in (Adam state reset) or out. */
+int prr_sg_trainer_set_params(prr_sg_trainer* t, const float* host_params);
+int prr_sg_trainer_get_params(prr_sg_trainer* t, float* host_params);
+/* The trainer's device parameters (for prr_develop_learned). */
+const float* prr_sg_trainer_device_params(prr_sg_trainer* t);
+/* One Adam step (beta 0.9 / 0.999); `crops` holds 3 * batch values; `loss`
+ * (nullable; when given the call waits) receives the batch's mean squared
+ * error before the step. */
+int prr_sg_trainer_step(prr_sg_trainer* t, const uint32_t* crops, float lr, float* loss);
+/* Forward, loss and parameter gradient of one explicit image: in16 [16][hq][wq],
+ * base3 [3][hq][wq], target3 [3][2hq][2wq] planar f32, host memory. For
+ * checking the device gradients. */
+int prr_sg_gradients(prr_ctx* ctx, const float* in16, const float* base3, const float* target3, uint32_t hq,
+                     uint32_t wq, const float* params, float* head_out, float* dparams, double* loss);
+
 /* --- host-buffer conveniences (synchronous) ----------------------------------- */
 /* decode_frame_with + develop_planar_into / develop_into with host input and
  * host outputs: uploads the packet, decodes and develops on the device and

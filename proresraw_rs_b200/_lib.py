@@ -141,6 +141,14 @@ class CBatchConfig(C.Structure):
     ]
 
 
+class CSgModel(C.Structure):
+    _fields_ = [
+        ("dev_params", C.c_void_p),
+        ("noise_lo", C.c_float),
+        ("noise_hi", C.c_float),
+    ]
+
+
 SCALE_FULL = 0
 
 _lib = None
@@ -200,6 +208,18 @@ def lib():
         "prr_batch_tune": (i, [vp, P(CJob), sz, C.c_uint32, P(CBatchConfig), P(C.c_float)]),
         "prr_batch_set_config": (i, [vp, C.c_uint32, P(CBatchConfig)]),
         "prr_batch_get_config": (i, [vp, C.c_uint32, P(CBatchConfig)]),
+        "prr_sg_param_count": (sz, []),
+        "prr_develop_learned": (i, [vp, P(CHeader), P(CParams), i, vp, P(CSgModel), i, vp, vp, vp, sz,
+                                    P(C.c_uint32)]),
+        "prr_sg_trainer_create": (i, [vp, C.c_uint32, C.c_uint32, P(vp)]),
+        "prr_sg_trainer_destroy": (None, [vp]),
+        "prr_sg_trainer_add_frame": (i, [vp, P(CHeader), P(CParams), vp, P(C.c_uint32)]),
+        "prr_sg_trainer_noise_range": (i, [vp, P(C.c_float), P(C.c_float)]),
+        "prr_sg_trainer_set_params": (i, [vp, vp]),
+        "prr_sg_trainer_get_params": (i, [vp, vp]),
+        "prr_sg_trainer_device_params": (vp, [vp]),
+        "prr_sg_trainer_step": (i, [vp, vp, C.c_float, P(C.c_float)]),
+        "prr_sg_gradients": (i, [vp, vp, vp, vp, C.c_uint32, C.c_uint32, vp, vp, vp, P(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -29,7 +29,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O3",
     "-shared",
 ]
-CUDA_SOURCES = ["api.cu", "batch.cu", "decode.cu", "develop.cu", "noalloc.cu"]
+CUDA_SOURCES = ["api.cu", "batch.cu", "decode.cu", "develop.cu", "learned.cu", "noalloc.cu"]
 CXX_FLAGS = ["-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-shared"]
 
 

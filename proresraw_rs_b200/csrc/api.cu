@@ -223,6 +223,8 @@ void prr_ctx_destroy(prr_ctx* c) {
     c->planes.release();
     batch_state_destroy(c->batch);
     c->batch = nullptr;
+    learned_state_destroy(c->learned);
+    c->learned = nullptr;
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -451,7 +453,9 @@ void params_wb(const prr_header* h, uint32_t quantizer, float red, float blue, p
     out->wb[1] = blue;
 }
 
-void output_matrix(const prr_header* h, int exposure, float* m) {
+}  // namespace
+
+void prr::output_matrix(const prr_header* h, int exposure, float* m) {
     // src/demosaic.rs:138-153, XYZ_TO_REC2020 from src/demosaic.rs:37-41.
     static const double G[3][3] = {{1.716651187971268, -0.355670783776393, -0.25336628137366},
                                    {-0.666684351832489, 1.616481236634939, 0.015768545813911},
@@ -466,9 +470,14 @@ void output_matrix(const prr_header* h, int exposure, float* m) {
     }
 }
 
-int develop_launch(prr_ctx* c, const prr_header* h, const prr_params* params, int stage,
-                   const uint16_t* dev_samples, int layout, float* r, float* g, float* b, size_t out_len) {
-    if (!c || !h || !params || !dev_samples || !r) return PRR_ERR_INVALID;
+namespace {
+
+}  // namespace
+
+// Check a develop call's arguments and fill its kernel descriptor.
+int prr::build_develop_desc(const prr_header* h, const prr_params* params, int stage, const uint16_t* dev_samples,
+                            int layout, float* r, float* g, float* b, size_t out_len, DevelopDesc* out) {
+    if (!h || !params || !dev_samples || !r) return PRR_ERR_INVALID;
     if (stage < PRR_STAGE_DEMOSAICED || stage > PRR_STAGE_REC2020) return PRR_ERR_INVALID;
     const size_t n = size_t(h->width) * h->height;
     if (layout == PRR_PLANAR) {
@@ -482,7 +491,6 @@ int develop_launch(prr_ctx* c, const prr_header* h, const prr_params* params, in
     } else {
         return PRR_ERR_INVALID;
     }
-    PRR_TRY(c->use_device());
     // Conversion::new, src/demosaic.rs:286-304.
     prr_params p = *params;
     if (stage == PRR_STAGE_DEMOSAICED) {
@@ -516,6 +524,18 @@ int develop_launch(prr_ctx* c, const prr_header* h, const prr_params* params, in
     d.r = r;
     d.g = g;
     d.b = b;
+    *out = d;
+    return PRR_OK;
+}
+
+namespace {
+
+int develop_launch(prr_ctx* c, const prr_header* h, const prr_params* params, int stage,
+                   const uint16_t* dev_samples, int layout, float* r, float* g, float* b, size_t out_len) {
+    if (!c) return PRR_ERR_INVALID;
+    DevelopDesc d{};
+    PRR_TRY(build_develop_desc(h, params, stage, dev_samples, layout, r, g, b, out_len, &d));
+    PRR_TRY(c->use_device());
     return c->cuda(launch_develop(d, c->stream));
 }
 

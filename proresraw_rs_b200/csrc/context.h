@@ -53,6 +53,8 @@ struct HostBuf {
 namespace prr {
 struct BatchState;  // batch.cu
 void batch_state_destroy(BatchState* b);
+struct LearnedState;  // learned.cu
+void learned_state_destroy(LearnedState* s);
 }  // namespace prr
 
 struct prr_ctx {
@@ -69,6 +71,7 @@ struct prr_ctx {
     DevBuf<uint16_t> samples;
     DevBuf<float> planes;
     prr::BatchState* batch = nullptr;
+    prr::LearnedState* learned = nullptr;
     std::string last_error;
 
     int cuda(cudaError_t e) {

@@ -156,6 +156,8 @@ struct DevShared {
 template <bool PRE>
 __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
     __shared__ DevShared S;
+    // Only the tiles a mask selects (the learned develop's fallback tiles).
+    if (d.tile_mask && !d.tile_mask[blockIdx.y * gridDim.x + blockIdx.x]) return;
     const int tid = threadIdx.x;
     const int w = d.w, h = d.h;
     const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;

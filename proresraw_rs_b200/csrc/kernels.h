@@ -132,7 +132,18 @@ struct DevelopDesc {
     float* r;
     float* g;
     float* b;
+    // Non-null: develop only the 32x32 tiles whose byte is nonzero (row-major
+    // over the tile grid).
+    const uint8_t* tile_mask;
 };
+
+constexpr int kDevelopTile = 32;
+
+// Argument checks and kernel descriptor of develop_into / develop_planar_into
+// (api.cu), and output_matrix (src/demosaic.rs:138-153).
+int build_develop_desc(const prr_header* h, const prr_params* params, int stage, const uint16_t* dev_samples,
+                       int layout, float* r, float* g, float* b, size_t out_len, DevelopDesc* out);
+void output_matrix(const prr_header* h, int exposure, float* m);
 
 cudaError_t launch_linearize(const uint16_t* codes, uint32_t stride, int w, int h,
                              const uint32_t* c0, const uint32_t* delta, uint16_t* out,

@@ -1,0 +1,1212 @@
+// learned.cu -- the learned demosaic surrogate: a small convolutional network
+// that develops a decoded frame to white-balanced (or Rec.2020) RGB, run on
+// the 5th-generation tensor cores, with its training on the device. No
+// counterpart in the crate: the plain develop (develop.cu) is its reference,
+// its training target and its per-tile fallback.
+//
+// Network (the CPU restatement in the oracle states the same):
+//  input   half resolution, one pixel per 2x2 Bayer quad, 16 channels. From
+//          the quad's red, two greens and blue (normalized linear values as
+//          the plain develop computes them, red and blue times their
+//          white-balance gains) and its mean green gm: 4 (each colour - gm),
+//          a noise channel 64 * sqrt of the plain develop's noise variance at
+//          gm, gm, 4 gx, 4 gy, 4 lap (half differences of the neighbouring
+//          quads' gm, east - west and south - north, and gm minus their mean;
+//          the quad grid clamped at its edges), 7 zero channels. The small
+//          differences keep in bf16 the detail the output needs;
+//  layers  conv 3x3 16->32, five conv 3x3 32->32 (bias, ReLU, bf16), head
+//          conv 3x3 32->16 (12 used; bias, f32); zero padding at every layer;
+//          bf16 products accumulated in f32 (tcgen05.mma kind::f16);
+//  output  head channel c*4 + 2*sy + sx of a quad plus the quad's colour
+//          (red, mean green, blue) is pixel (2i + sx, 2j + sy); min(., 1), then
+//          the Rec.2020 matrix for that stage.
+//
+// Data layouts: activations bf16 in channel chunks, [image][C/8][H][W][8]
+// (16 bytes per pixel and chunk: a run of 8 pixels of one chunk is one
+// 8 x 16-byte core matrix of the tensor core's K-major operand layout);
+// head, gradients and colours f32 planar [image][C][H][W].
+//
+// Convolution on the tensor cores: one CTA computes a 32 x 16 pixel tile as
+// four M = 128 blocks (8 columns x 16 rows each). The input window (34 x 18
+// pixels, all chunks) and the layer's weights are staged in shared memory;
+// for each block, tap and 16-channel half, one thread issues
+// tcgen05.mma.cta_group::1.kind::f16 with M = 128, N = cout, K = 16: A is the
+// window shifted by the tap (start address moves by the tap's offset; the
+// next 8 rows of M are the next window row, the second K chunk the next
+// chunk plane), B the tap's weights [cout][16]. Accumulators live in tensor
+// memory (4 x cout columns); tcgen05.commit signals an mbarrier; each warp
+// reads its 32 lanes back with tcgen05.ld, adds the bias, applies ReLU and
+// stores bf16 chunks (or the f32 head).
+//
+// Backward (training only) runs on the CUDA cores in f32: the gradient of
+// each layer's input through the ReLU, and weight and bias gradients reduced
+// per CTA and added with atomics. Adam keeps f32 master weights; the tensor
+// core copy is re-packed to bf16 before each forward.
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/prr.h"
+#include "context.h"
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace prr {
+namespace sg {
+
+constexpr int kIn = 16, kHid = 32, kHead = 16, kLayers = 7;
+__host__ __device__ constexpr int cin_of(int l) { return l == 0 ? kIn : kHid; }
+__host__ __device__ constexpr int cout_of(int l) { return l == kLayers - 1 ? kHead : kHid; }
+__host__ __device__ constexpr size_t layer_off(int l) {
+    size_t off = 0;
+    for (int k = 0; k < l; k++) off += size_t(cout_of(k)) * cin_of(k) * 9 + cout_of(k);
+    return off;
+}
+__host__ __device__ constexpr size_t packed_off(int l) {  // bf16 elements
+    size_t off = 0;
+    for (int k = 0; k < l; k++) off += size_t(9) * cin_of(k) * cout_of(k);
+    return off;
+}
+constexpr size_t kParams = layer_off(kLayers);
+constexpr size_t kPacked = packed_off(kLayers);
+
+constexpr int TX = 32, TY = 16;          // output tile of a conv CTA
+constexpr int WX = TX + 2, WY = TY + 2;  // input window
+constexpr int kConvThreads = 128;
+constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
+
+template <int CIN, int COUT>
+struct ConvCfg {
+    static constexpr int C8 = CIN / 8;
+    static constexpr int CS = WY * WX * 16;  // bytes per chunk plane of the window
+    static constexpr int RP = WX * 16;       // bytes per window row
+    static constexpr int WIN_BYTES = C8 * CS;
+    static constexpr int W_BYTES = 9 * C8 * COUT * 16;
+    static constexpr int SMEM = WIN_BYTES + W_BYTES;
+    static constexpr uint32_t TMEM_COLS = 4 * COUT;
+    // Instruction descriptor, kind::f16: f32 accumulator (bits 4-5 = 1), A
+    // and B bf16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17,
+    // M >> 4 at bit 24.
+    static constexpr uint32_t IDESC =
+        (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(COUT >> 3) << 17) | (uint32_t(128 >> 4) << 24);
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "tcgen05 shape");
+};
+
+struct ConvArgs {
+    const uint4* x;     // bf16 chunks [image][CIN/8][H][W]
+    const uint4* w;     // the layer's packed weights [tap][CIN/8][COUT] x 8 bf16
+    const float* bias;  // [COUT]
+    uint4* y;           // hidden layers: bf16 chunks [image][COUT/8][H][W]
+    float* yf;          // head: f32 [image][16][H][W]
+    const int4* valid;  // per image: x0, y0, x1, y1 (null: the whole image)
+    int H, W;
+    unsigned* error;    // bit 0: a tensor-core wait ran out of time
+};
+
+// --- tcgen05 / mbarrier helpers ------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, no swizzle: start address, leading byte
+// offset (between the two 8-element K chunks), stride byte offset (between
+// 8-row groups of M or N), descriptor version 1 at bit 46.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((addr & 0x3FFFFu) >> 4) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait for phase `parity` of the mbarrier, for at most ~limit_ns and a fixed
+// number of polls.
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint64_t limit_ns) {
+    if (mbar_try_wait(mbar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 0; i < (1u << 24); i++) {
+        if (mbar_try_wait(mbar, parity)) return true;
+        __nanosleep(64);
+        if (global_ns() - t0 > limit_ns) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+#define SG_R8(i) "=r"(v[i + 0]), "=r"(v[i + 1]), "=r"(v[i + 2]), "=r"(v[i + 3]), "=r"(v[i + 4]), \
+                 "=r"(v[i + 5]), "=r"(v[i + 6]), "=r"(v[i + 7])
+
+// 32 lanes x N f32 columns of tensor memory into registers (lane = thread).
+template <int N>
+__device__ __forceinline__ void tmem_load(uint32_t taddr, uint32_t* v);
+template <>
+__device__ __forceinline__ void tmem_load<32>(uint32_t taddr, uint32_t* v) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : SG_R8(0), SG_R8(8), SG_R8(16), SG_R8(24)
+        : "r"(taddr));
+}
+template <>
+__device__ __forceinline__ void tmem_load<16>(uint32_t taddr, uint32_t* v) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : SG_R8(0), SG_R8(8)
+        : "r"(taddr));
+}
+#undef SG_R8
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+    const __nv_bfloat16 a = __float2bfloat16_rn(lo), b = __float2bfloat16_rn(hi);
+    return uint32_t(__bfloat16_as_ushort(a)) | (uint32_t(__bfloat16_as_ushort(b)) << 16);
+}
+
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xFFFF0000u); }
+
+__device__ __forceinline__ bool in_valid(const int4* valid, int b, int x, int y) {
+    if (!valid) return true;
+    const int4 v = valid[b];
+    return x >= v.x && y >= v.y && x < v.z && y < v.w;
+}
+
+// --- the convolution on the tensor cores --------------------------------------
+
+template <int CIN, int COUT, bool HEAD>
+__global__ void __launch_bounds__(kConvThreads) k_sg_conv(ConvArgs a) {
+    using C = ConvCfg<CIN, COUT>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int img = blockIdx.z;
+    const int tx0 = blockIdx.x * TX, ty0 = blockIdx.y * TY;
+    uint8_t* win = smem;
+    uint8_t* wsm = smem + C::WIN_BYTES;
+
+    // Window (zero outside the image) and weights, 16 bytes per access.
+    const uint4* xb = a.x + size_t(img) * C::C8 * a.H * a.W;
+    for (int v = tid; v < C::C8 * WY * WX; v += kConvThreads) {
+        const int c = v / (WY * WX), r = (v / WX) % WY, q = v % WX;
+        const int gy = ty0 - 1 + r, gx = tx0 - 1 + q;
+        uint4 val = make_uint4(0, 0, 0, 0);
+        if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W) val = __ldg(xb + (size_t(c) * a.H + gy) * a.W + gx);
+        *reinterpret_cast<uint4*>(win + c * C::CS + r * C::RP + q * 16) = val;
+    }
+    for (int v = tid; v < C::W_BYTES / 16; v += kConvThreads) reinterpret_cast<uint4*>(wsm)[v] = __ldg(a.w + v);
+    // Generic-proxy stores become visible to the tensor core's reads.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(C::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t bar = smem_u32(&mbar);
+
+    if (tid == 0) {
+        const uint32_t win_a = smem_u32(win), w_a = smem_u32(wsm);
+#pragma unroll 1
+        for (int bk = 0; bk < 4; bk++) {
+#pragma unroll 1
+            for (int t = 0; t < 9; t++) {
+                const int dy = t / 3, dx = t % 3;
+#pragma unroll
+                for (int h = 0; h < C::C8 / 2; h++) {
+                    // A: rows m = 8 * r + i are window pixel (r + dy, 8 bk + i + dx),
+                    // K chunk k = the window's chunk plane 2 h + k.
+                    const uint32_t aa = win_a + uint32_t((2 * h) * C::CS + dy * C::RP + (8 * bk + dx) * 16);
+                    // B: rows n = output channel, K chunk k = weights of input
+                    // channels 16 h + 8 k .. + 7 at this tap.
+                    const uint32_t ba = w_a + uint32_t((t * C::C8 + 2 * h) * COUT * 16);
+                    umma_f16(tmem + uint32_t(bk * COUT), sdesc(aa, C::CS, C::RP), sdesc(ba, COUT * 16, 128),
+                             C::IDESC, (t | h) != 0 ? 1u : 0u);
+                }
+            }
+        }
+        umma_commit(bar);
+    }
+    // The epilogue's tensor-memory loads are warp-collective: every thread
+    // takes the same branch.
+    const bool ok = __syncthreads_and(mbar_wait(bar, 0, kWaitNs) ? 1 : 0) != 0;
+    if (!ok) {
+        if (tid == 0) atomicOr(a.error, 1u);
+        mbar_wait(bar, 0, kWaitNs);  // let the issued work finish before the memory is freed
+    }
+    tc_fence_after();
+    if (ok) {
+        const int m = 32 * warp + lane;  // accumulator row of this thread
+        const int py = ty0 + (m >> 3);
+#pragma unroll 1
+        for (int bk = 0; bk < 4; bk++) {
+            const int px = tx0 + 8 * bk + (m & 7);
+            uint32_t v[COUT];
+            tmem_load<COUT>(tmem + (uint32_t(32 * warp) << 16) + uint32_t(bk * COUT), v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (py >= a.H || px >= a.W) continue;
+            const bool keep = in_valid(a.valid, img, px, py);
+            if (HEAD) {
+                float* o = a.yf + (size_t(img) * kHead * a.H + py) * a.W + px;
+#pragma unroll
+                for (int c = 0; c < COUT; c++)
+                    o[size_t(c) * a.H * a.W] = keep ? __fadd_rn(__uint_as_float(v[c]), __ldg(a.bias + c)) : 0.0f;
+            } else {
+                uint4* o = a.y + (size_t(img) * (COUT / 8) * a.H + py) * a.W + px;
+#pragma unroll
+                for (int c8 = 0; c8 < COUT / 8; c8++) {
+                    float f[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e++) {
+                        const float s = __fadd_rn(__uint_as_float(v[c8 * 8 + e]), __ldg(a.bias + c8 * 8 + e));
+                        f[e] = keep ? fmaxf(s, 0.0f) : 0.0f;
+                    }
+                    o[size_t(c8) * a.H * a.W] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
+                                                           pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::TMEM_COLS));
+}
+
+template <int CIN, int COUT, bool HEAD>
+cudaError_t conv_launch(const ConvArgs& a, int images, cudaStream_t s) {
+    using C = ConvCfg<CIN, COUT>;
+    static bool attr = false;  // per process; the attribute is per device and set on first use
+    if (!attr) {
+        const cudaError_t e = cudaFuncSetAttribute(k_sg_conv<CIN, COUT, HEAD>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    dim3 grid((a.W + TX - 1) / TX, (a.H + TY - 1) / TY, images);
+    k_sg_conv<CIN, COUT, HEAD><<<grid, kConvThreads, C::SMEM, s>>>(a);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// --- input packing, weights, output ------------------------------------------------
+
+struct PackArgs {
+    const uint16_t* codes;
+    uint32_t stride;
+    int w, h, wq, hq;
+    uint32_t c0[8], cd[8];
+    int rr, rc, black;
+    float one_over_range, bs, wb0, wb1;
+    float n0, n1, n2;
+    uint4* in;      // [2][hq][wq] chunks
+    float* base;    // [3][hq][wq]
+    float* noise_minmax;  // optional: atomic min / max of the noise channel (as ordered ints)
+};
+
+__device__ __forceinline__ float sg_nrm(const PackArgs& p, int x, int y) {
+    x = min(x, p.w - 1);
+    y = min(y, p.h - 1);
+    const uint32_t lin = curve_apply(p.c0, p.cd, p.codes[size_t(y) * p.stride + x]);
+    return __fmul_rn(p.one_over_range, float(int32_t(lin) - p.black));
+}
+
+// Mean green of quad (i, j), the quad grid clamped at its edges.
+__device__ __forceinline__ float sg_green(const PackArgs& p, int i, int j) {
+    i = min(max(i, 0), p.wq - 1);
+    j = min(max(j, 0), p.hq - 1);
+    const float gr = sg_nrm(p, 2 * i + 1 - p.rc, 2 * j + p.rr);
+    const float gb = sg_nrm(p, 2 * i + p.rc, 2 * j + 1 - p.rr);
+    return __fmul_rn(__fadd_rn(gr, gb), 0.5f);
+}
+
+__global__ void k_sg_pack(PackArgs p) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= p.wq) return;
+    const int x0 = 2 * i, y0 = 2 * j;
+    const float r = __fmul_rn(sg_nrm(p, x0 + p.rc, y0 + p.rr), p.wb0);
+    const float gr = sg_nrm(p, x0 + 1 - p.rc, y0 + p.rr);
+    const float gb = sg_nrm(p, x0 + p.rc, y0 + 1 - p.rr);
+    const float b = __fmul_rn(sg_nrm(p, x0 + 1 - p.rc, y0 + 1 - p.rr), p.wb1);
+    const float gm = __fmul_rn(__fadd_rn(gr, gb), 0.5f);
+    const float t = __fadd_rn(p.bs, gm);
+    const float var = __fadd_rn(p.n2, fmaxf(p.n1, __fmul_rn(p.n0, __fmul_rn(t, t))));
+    const float noise = __fmul_rn(64.0f, __fsqrt_rn(var));
+    const float ge = sg_green(p, i + 1, j), gw = sg_green(p, i - 1, j);
+    const float gs = sg_green(p, i, j + 1), gn = sg_green(p, i, j - 1);
+    const float gx = __fmul_rn(__fsub_rn(ge, gw), 0.5f), gy = __fmul_rn(__fsub_rn(gs, gn), 0.5f);
+    const float lap = __fsub_rn(gm, __fmul_rn(__fadd_rn(__fadd_rn(ge, gw), __fadd_rn(gs, gn)), 0.25f));
+    auto d4 = [](float v, float ref) { return __fmul_rn(__fsub_rn(v, ref), 4.0f); };
+    const size_t q = size_t(j) * p.wq + i, plane = size_t(p.wq) * p.hq;
+    p.in[q] = make_uint4(pack_bf16x2(d4(r, gm), d4(gr, gm)), pack_bf16x2(d4(gb, gm), d4(b, gm)),
+                         pack_bf16x2(noise, gm), pack_bf16x2(__fmul_rn(gx, 4.0f), __fmul_rn(gy, 4.0f)));
+    p.in[plane + q] = make_uint4(pack_bf16x2(__fmul_rn(lap, 4.0f), 0.0f), 0u, 0u, 0u);
+    p.base[q] = r;
+    p.base[plane + q] = gm;
+    p.base[2 * plane + q] = b;
+    if (p.noise_minmax) {
+        // The noise channel as the network sees it (bf16), as a non-negative
+        // float whose bits order like ints.
+        const float nb = bf16_lo(pack_bf16x2(noise, 0.0f));
+        atomicMin(reinterpret_cast<int*>(p.noise_minmax), __float_as_int(nb));
+        atomicMax(reinterpret_cast<int*>(p.noise_minmax) + 1, __float_as_int(nb));
+    }
+}
+
+// f32 parameters -> bf16 weights in the tensor cores' B layout, all layers.
+__global__ void k_sg_pack_weights(const float* __restrict__ params, uint16_t* __restrict__ packed) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= kPacked) return;
+    int l = 0;
+    while (l < kLayers - 1 && i >= packed_off(l + 1)) l++;
+    const int cin = cin_of(l), cout = cout_of(l);
+    const size_t k = i - packed_off(l);
+    // k = ((tap * cin/8 + kc) * cout + n) * 8 + e
+    const int e = int(k % 8), n = int((k / 8) % cout);
+    const int kc = int((k / 8 / cout) % (cin / 8)), tap = int(k / 8 / cout / (cin / 8));
+    const float wv = params[layer_off(l) + (size_t(n) * cin + kc * 8 + e) * 9 + tap];
+    packed[i] = __bfloat16_as_ushort(__float2bfloat16_rn(wv));
+}
+
+struct OutArgs {
+    const float* head;  // [16][hq][wq]
+    const float* base;  // [3][hq][wq]
+    int w, h, wq, hq;
+    int has_matrix;
+    float m[9];
+    int layout;
+    float* r;
+    float* g;
+    float* b;
+    const uint8_t* fallback;  // per 32x32 tile: developed by the plain kernel instead
+    int tiles_x;
+};
+
+__global__ void k_sg_output(OutArgs o) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= o.w) return;
+    if (o.fallback && o.fallback[(y / kDevelopTile) * o.tiles_x + x / kDevelopTile]) return;
+    const size_t plane = size_t(o.wq) * o.hq;
+    const size_t q = size_t(y >> 1) * o.wq + (x >> 1);
+    const int s = (y & 1) * 2 + (x & 1);
+    float r = fminf(__fadd_rn(o.head[(0 + s) * plane + q], o.base[q]), 1.0f);
+    float g = fminf(__fadd_rn(o.head[(4 + s) * plane + q], o.base[plane + q]), 1.0f);
+    float b = fminf(__fadd_rn(o.head[(8 + s) * plane + q], o.base[2 * plane + q]), 1.0f);
+    if (o.has_matrix) {
+        const float r0 = r, g0 = g, b0 = b;
+        r = __fmaf_rn(b0, o.m[2], __fmaf_rn(r0, o.m[0], __fmul_rn(g0, o.m[1])));
+        g = __fmaf_rn(b0, o.m[5], __fmaf_rn(r0, o.m[3], __fmul_rn(g0, o.m[4])));
+        b = __fmaf_rn(b0, o.m[8], __fmaf_rn(r0, o.m[6], __fmul_rn(g0, o.m[7])));
+    }
+    const size_t i = size_t(y) * o.w + x;
+    if (o.layout == PRR_PLANAR) {
+        o.r[i] = r;
+        o.g[i] = g;
+        o.b[i] = b;
+    } else {
+        o.r[3 * i] = r;
+        o.r[3 * i + 1] = g;
+        o.r[3 * i + 2] = b;
+    }
+}
+
+// Per 32x32 output tile: does any quad's noise channel leave [lo, hi]?
+__global__ void k_sg_fallback(const uint4* __restrict__ in, int wq, int hq, int tiles_x, float lo, float hi,
+                              uint8_t* __restrict__ mask, unsigned* __restrict__ count) {
+    const int tile = blockIdx.x;
+    const int qx0 = (tile % tiles_x) * (kDevelopTile / 2), qy0 = (tile / tiles_x) * (kDevelopTile / 2);
+    const int u = threadIdx.x % 16, v = threadIdx.x / 16;
+    int out = 0;
+    if (qx0 + u < wq && qy0 + v < hq) {
+        const float n = bf16_lo(in[size_t(qy0 + v) * wq + qx0 + u].z);
+        out = (n < lo || n > hi) ? 1 : 0;
+    }
+    out = __syncthreads_or(out);
+    if (threadIdx.x == 0) {
+        mask[tile] = uint8_t(out);
+        if (out) atomicAdd(count, 1u);
+    }
+}
+
+// --- training ------------------------------------------------------------------------
+
+struct GatherItem {
+    const uint4* in;      // frame input chunks [2][hq][wq]
+    const float* base;    // [3][hq][wq]
+    const float* target;  // plain develop, white-balanced, planar [3][h][w]
+    int w, h, wq, hq;
+    int cx, cy;           // crop origin, full resolution, even
+};
+
+// Window u, v of image k is frame quad (cx/2 - margin + u, cy/2 - margin + v).
+__global__ void k_sg_gather(const GatherItem* __restrict__ items, int hw, int ww, int margin, int crop,
+                            uint4* __restrict__ in, float* __restrict__ base, float* __restrict__ target,
+                            int4* __restrict__ valid) {
+    const int k = blockIdx.z;
+    const GatherItem it = items[k];
+    const int u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y;
+    const int qx0 = it.cx / 2 - margin, qy0 = it.cy / 2 - margin;
+    const size_t wplane = size_t(hw) * ww, fplane = size_t(it.wq) * it.hq;
+    if (u < ww) {
+        const int fx = qx0 + u, fy = qy0 + v;
+        const bool inside = fx >= 0 && fy >= 0 && fx < it.wq && fy < it.hq;
+        const size_t wi = size_t(k) * 2 * wplane + size_t(v) * ww + u;
+        const size_t fi = size_t(fy) * it.wq + fx;
+        in[wi] = inside ? it.in[fi] : make_uint4(0, 0, 0, 0);
+        in[wi + wplane] = inside ? it.in[fplane + fi] : make_uint4(0, 0, 0, 0);
+        for (int c = 0; c < 3; c++)
+            base[(size_t(k) * 3 + c) * wplane + size_t(v) * ww + u] = inside ? it.base[c * fplane + fi] : 0.0f;
+    }
+    // Target crop: rows 2v, 2v+1 of the crop, columns 2u, 2u+1.
+    if (u < crop / 2 && v < crop / 2) {
+        for (int dy = 0; dy < 2; dy++)
+            for (int dx = 0; dx < 2; dx++) {
+                const int x = 2 * u + dx, y = 2 * v + dy;
+                const size_t fi = size_t(it.cy + y) * it.w + it.cx + x;
+                for (int c = 0; c < 3; c++)
+                    target[((size_t(k) * 3 + c) * crop + y) * crop + x] = it.target[size_t(c) * it.w * it.h + fi];
+            }
+    }
+    if (u == 0 && v == 0 && threadIdx.x == 0) {
+        valid[k] = make_int4(max(0, -qx0), max(0, -qy0), min(ww, it.wq - qx0), min(hw, it.hq - qy0));
+    }
+}
+
+// Loss over the crop (full resolution, at window quad offset `margin`) and
+// its gradient with respect to the head. dhead must be zero beforehand.
+__global__ void k_sg_loss(const float* __restrict__ head, const float* __restrict__ base,
+                          const float* __restrict__ target, int hw, int ww, int margin, int cw, int ch, float scale,
+                          float* __restrict__ dhead, double* __restrict__ loss) {
+    const int k = blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    float local = 0.0f;
+    if (x < cw && y < ch) {
+        const size_t wplane = size_t(hw) * ww;
+        const size_t q = size_t(margin + (y >> 1)) * ww + margin + (x >> 1);
+        const int s = (y & 1) * 2 + (x & 1);
+        for (int c = 0; c < 3; c++) {
+            const size_t hi = (size_t(k) * kHead + c * 4 + s) * wplane + q;
+            const float out = head[hi] + base[(size_t(k) * 3 + c) * wplane + q];
+            const float d = out - target[((size_t(k) * 3 + c) * ch + y) * cw + x];
+            local += d * d;
+            dhead[hi] = 2.0f * d * scale;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) local += __shfl_xor_sync(0xFFFFFFFFu, local, o);
+    __shared__ float part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = local;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.0f;
+        for (int i = 0; i < int(blockDim.x / 32); i++) s += part[i];
+        atomicAdd(loss, double(s));
+    }
+}
+
+// Gradient of a layer's input through the ReLU that produced it:
+// dx[ci] = (x[ci] > 0) * sum_{co, tap} W[co][ci][tap] dy[co][p - tap].
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) k_sg_dx(const float* __restrict__ dy, const float* __restrict__ w,
+                                               const uint4* __restrict__ x, int H, int W, float* __restrict__ dx) {
+    __shared__ float ws[COUT * 9 * CIN];  // [co][tap][ci]
+    for (int i = threadIdx.x; i < COUT * 9 * CIN; i += blockDim.x) {
+        const int ci = i % CIN, t = (i / CIN) % 9, co = i / (CIN * 9);
+        ws[i] = w[(size_t(co) * CIN + ci) * 9 + t];
+    }
+    __syncthreads();
+    const int img = blockIdx.z;
+    const int px = blockIdx.x * 32 + (threadIdx.x & 31), py = blockIdx.y * 4 + (threadIdx.x >> 5);
+    if (px >= W || py >= H) return;
+    const size_t plane = size_t(H) * W;
+    float acc[CIN];
+#pragma unroll
+    for (int i = 0; i < CIN; i++) acc[i] = 0.0f;
+    for (int co = 0; co < COUT; co++) {
+        const float* dyc = dy + (size_t(img) * COUT + co) * plane;
+#pragma unroll
+        for (int t = 0; t < 9; t++) {
+            const int oy = py - (t / 3 - 1), ox = px - (t % 3 - 1);
+            if (oy < 0 || oy >= H || ox < 0 || ox >= W) continue;
+            const float g = __ldg(dyc + size_t(oy) * W + ox);
+            const float* wr = ws + (co * 9 + t) * CIN;
+#pragma unroll
+            for (int ci = 0; ci < CIN; ci++) acc[ci] = fmaf(wr[ci], g, acc[ci]);
+        }
+    }
+    const size_t p = size_t(py) * W + px;
+#pragma unroll
+    for (int c8 = 0; c8 < CIN / 8; c8++) {
+        const uint4 xv = __ldg(x + (size_t(img) * (CIN / 8) + c8) * plane + p);
+        const uint32_t words[4] = {xv.x, xv.y, xv.z, xv.w};
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const float xe = (e & 1) ? bf16_hi(words[e >> 1]) : bf16_lo(words[e >> 1]);
+            dx[(size_t(img) * CIN + c8 * 8 + e) * plane + p] = xe > 0.0f ? acc[c8 * 8 + e] : 0.0f;
+        }
+    }
+}
+
+// Weight and bias gradients: thread (co group, ci) accumulates CO_T output
+// channels x 9 taps over the CTA's tiles of 32 x 8 pixels, then adds them.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(128) k_sg_dw(const float* __restrict__ dy, const uint4* __restrict__ x, int H,
+                                               int W, int images, float* __restrict__ dw, float* __restrict__ db) {
+    constexpr int CO_T = COUT * CIN / 128;
+    // Pixel tile 32 x 4; the input with its halo, 6 x 34 per channel, padded
+    // to an odd stride so that the 32 channels of a warp fall in 32 banks.
+    constexpr int PX = 32, PY = 4, XR = PY + 2, XC = PX + 2, XS = XR * XC + 1;
+    __shared__ float xs[CIN * XS];
+    __shared__ float ds[COUT * PX * PY];
+    const int tid = threadIdx.x;
+    const int ci = tid % CIN, cog = tid / CIN;
+    float acc[CO_T][9];
+    float bacc[CO_T];
+#pragma unroll
+    for (int a = 0; a < CO_T; a++) {
+        bacc[a] = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 9; t++) acc[a][t] = 0.0f;
+    }
+    const int tiles_x = (W + PX - 1) / PX, tiles_y = (H + PY - 1) / PY;
+    const int ntiles = tiles_x * tiles_y * images;
+    const size_t plane = size_t(H) * W;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int img = tile / (tiles_x * tiles_y), rem = tile % (tiles_x * tiles_y);
+        const int x0 = (rem % tiles_x) * PX, y0 = (rem / tiles_x) * PY;
+        __syncthreads();
+        for (int i = tid; i < (CIN / 8) * XR * XC; i += 128) {
+            const int c8 = i / (XR * XC), r = (i / XC) % XR, q = i % XC;
+            const int gy = y0 - 1 + r, gx = x0 - 1 + q;
+            uint4 v = make_uint4(0, 0, 0, 0);
+            if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(x + (size_t(img) * (CIN / 8) + c8) * plane + size_t(gy) * W + gx);
+            const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int e = 0; e < 8; e++)
+                xs[(c8 * 8 + e) * XS + r * XC + q] = (e & 1) ? bf16_hi(words[e >> 1]) : bf16_lo(words[e >> 1]);
+        }
+        for (int i = tid; i < COUT * PX * PY; i += 128) {
+            const int co = i / (PX * PY), r = (i / PX) % PY, q = i % PX;
+            const int gy = y0 + r, gx = x0 + q;
+            ds[i] = (gy < H && gx < W) ? __ldg(dy + (size_t(img) * COUT + co) * plane + size_t(gy) * W + gx) : 0.0f;
+        }
+        __syncthreads();
+        for (int r = 0; r < PY; r++)
+            for (int q = 0; q < PX; q++) {
+                float xv[9];
+#pragma unroll
+                for (int t = 0; t < 9; t++) xv[t] = xs[ci * XS + (r + t / 3) * XC + q + t % 3];
+#pragma unroll
+                for (int a = 0; a < CO_T; a++) {
+                    const float g = ds[(cog * CO_T + a) * PX * PY + r * PX + q];
+                    bacc[a] += g;
+#pragma unroll
+                    for (int t = 0; t < 9; t++) acc[a][t] = fmaf(xv[t], g, acc[a][t]);
+                }
+            }
+    }
+#pragma unroll
+    for (int a = 0; a < CO_T; a++) {
+        const int co = cog * CO_T + a;
+#pragma unroll
+        for (int t = 0; t < 9; t++) atomicAdd(dw + (size_t(co) * CIN + ci) * 9 + t, acc[a][t]);
+        if (ci == 0) atomicAdd(db + co, bacc[a]);
+    }
+}
+
+__global__ void k_sg_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, size_t n, float lr_t, float b1, float b2, float eps) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr_t * mi / (sqrtf(vi) + eps);
+}
+
+// Input chunks from planar f32 (the explicit-image gradient path).
+__global__ void k_sg_from_planar(const float* __restrict__ src, int plane, uint4* __restrict__ dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= plane) return;
+    for (int c8 = 0; c8 < 2; c8++) {
+        float f[8];
+        for (int e = 0; e < 8; e++) f[e] = src[size_t(c8 * 8 + e) * plane + i];
+        dst[size_t(c8) * plane + i] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
+                                                 pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
+    }
+}
+
+// --- host-side network passes ---------------------------------------------------------
+
+// Buffers of one forward over `images` images of hq x wq pixels.
+struct NetBuffers {
+    uint4* in = nullptr;      // [images][2][hq][wq]
+    uint4* act[6] = {};       // [images][4][hq][wq]
+    float* head = nullptr;    // [images][16][hq][wq]
+};
+
+cudaError_t forward(const NetBuffers& nb, const uint16_t* packed, const float* params, const int4* valid, int images,
+                    int hq, int wq, unsigned* error, cudaStream_t s) {
+    ConvArgs a{};
+    a.H = hq;
+    a.W = wq;
+    a.valid = valid;
+    a.error = error;
+    for (int l = 0; l < kLayers; l++) {
+        a.x = l == 0 ? nb.in : nb.act[l - 1];
+        a.w = reinterpret_cast<const uint4*>(packed + packed_off(l));
+        a.bias = params + layer_off(l) + size_t(cout_of(l)) * cin_of(l) * 9;
+        cudaError_t e;
+        if (l == 0) {
+            a.y = nb.act[0];
+            e = conv_launch<kIn, kHid, false>(a, images, s);
+        } else if (l < kLayers - 1) {
+            a.y = nb.act[l];
+            e = conv_launch<kHid, kHid, false>(a, images, s);
+        } else {
+            a.y = nullptr;
+            a.yf = nb.head;
+            e = conv_launch<kHid, kHead, true>(a, images, s);
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t pack_weights(const float* params, uint16_t* packed, cudaStream_t s) {
+    k_sg_pack_weights<<<unsigned((kPacked + 255) / 256), 256, 0, s>>>(params, packed);
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Backward from dhead: parameter gradients into grad (zeroed here).
+cudaError_t backward(const NetBuffers& nb, const float* params, const float* dhead, float* grad, float* d0, float* d1,
+                     int images, int hq, int wq, int sms, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(grad, 0, kParams * sizeof(float), s);
+    if (e != cudaSuccess) return e;
+    const float* dy = dhead;
+    float* bufs[2] = {d0, d1};
+    const dim3 gdx((wq + 31) / 32, (hq + 3) / 4, images);
+    const int gdw = std::max(1, sms * 4);
+    for (int l = kLayers - 1; l >= 0; l--) {
+        const uint4* x = l == 0 ? nb.in : nb.act[l - 1];
+        float* dw = grad + layer_off(l);
+        float* db = dw + size_t(cout_of(l)) * cin_of(l) * 9;
+        const float* w = params + layer_off(l);
+        float* dx = bufs[l & 1];
+        if (l == kLayers - 1) {
+            k_sg_dw<kHid, kHead><<<gdw, 128, 0, s>>>(dy, x, hq, wq, images, dw, db);
+            k_sg_dx<kHid, kHead><<<gdx, 128, 0, s>>>(dy, w, x, hq, wq, dx);
+            count_launch(2);
+        } else if (l > 0) {
+            k_sg_dw<kHid, kHid><<<gdw, 128, 0, s>>>(dy, x, hq, wq, images, dw, db);
+            k_sg_dx<kHid, kHid><<<gdx, 128, 0, s>>>(dy, w, x, hq, wq, dx);
+            count_launch(2);
+        } else {
+            k_sg_dw<kIn, kHid><<<gdw, 128, 0, s>>>(dy, x, hq, wq, images, dw, db);
+            count_launch();
+        }
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        dy = dx;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace sg
+
+// Per-context state of the learned develop: scratch and packed weights.
+struct LearnedState {
+    DevBuf<uint8_t> scratch;
+    DevBuf<uint16_t> packed;
+    DevBuf<unsigned> counters;  // [0] fallback tiles, [1] error
+    HostBuf<unsigned> hcounters;
+};
+
+void learned_state_destroy(LearnedState* s) {
+    if (!s) return;
+    s->scratch.release();
+    s->packed.release();
+    s->counters.release();
+    s->hcounters.release();
+    delete s;
+}
+
+}  // namespace prr
+
+// ---------------------------------------------------------------------------
+// Trainer.
+
+struct prr_sg_trainer {
+    prr_ctx* ctx = nullptr;
+    uint32_t batch = 0, crop = 0, margin = 8;
+    int sms = 0;
+    struct Frame {
+        DevBuf<uint4> in;
+        DevBuf<float> base;
+        DevBuf<float> target;
+        int w = 0, h = 0, wq = 0, hq = 0;
+    };
+    std::vector<Frame*> frames;
+    DevBuf<float> params, grad, m, v, minmax;
+    DevBuf<uint16_t> packed;
+    DevBuf<uint4> win_in;
+    DevBuf<uint4> acts;
+    DevBuf<float> base, target, head, dhead, d0, d1;
+    DevBuf<int4> valid;
+    DevBuf<prr::sg::GatherItem> items;
+    HostBuf<prr::sg::GatherItem> hitems;
+    DevBuf<double> loss;
+    DevBuf<unsigned> error;
+    HostBuf<double> hloss;
+    HostBuf<unsigned> herror;
+    HostBuf<float> hminmax;
+    uint32_t step = 0;
+    float noise_lo = 0.f, noise_hi = 0.f;
+    bool have_range = false;
+};
+
+using namespace prr;
+
+namespace {
+
+int learned_state(prr_ctx* c, LearnedState** out) {
+    if (!c->learned) c->learned = new LearnedState;
+    *out = c->learned;
+    return PRR_OK;
+}
+
+// Pack a decoded frame into the surrogate input and colours.
+int pack_frame(prr_ctx* c, const DevelopDesc& d, uint4* in, float* base, float* minmax) {
+    sg::PackArgs p{};
+    p.codes = d.codes;
+    p.stride = d.stride;
+    p.w = d.w;
+    p.h = d.h;
+    p.wq = (d.w + 1) / 2;
+    p.hq = (d.h + 1) / 2;
+    for (int i = 0; i < 8; i++) {
+        p.c0[i] = d.curve_c0[i];
+        p.cd[i] = d.curve_delta[i];
+    }
+    p.rr = d.cfa >> 1;
+    p.rc = d.cfa & 1;
+    p.black = d.black;
+    p.one_over_range = d.one_over_range;
+    p.bs = d.green_off;
+    p.wb0 = d.wb[0];
+    p.wb1 = d.wb[1];
+    p.n0 = d.noise[0];
+    p.n1 = d.noise[1];
+    p.n2 = d.noise[2];
+    p.in = in;
+    p.base = base;
+    p.noise_minmax = minmax;
+    dim3 grid((p.wq + 127) / 128, p.hq);
+    sg::k_sg_pack<<<grid, 128, 0, c->stream>>>(p);
+    count_launch();
+    return c->cuda(cudaGetLastError());
+}
+
+size_t up256(size_t v) { return (v + 255) & ~size_t(255); }
+
+}  // namespace
+
+extern "C" {
+
+size_t prr_sg_param_count(void) { return sg::kParams; }
+
+int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* params, int stage,
+                        const uint16_t* dev_samples, const prr_sg_model* model, int layout, float* r, float* g,
+                        float* b, size_t out_len, uint32_t* fallback_tiles) {
+    if (!c || !model || !model->dev_params) return PRR_ERR_INVALID;
+    DevelopDesc d{};
+    PRR_TRY(build_develop_desc(h, params, stage, dev_samples, layout, r, g, b, out_len, &d));
+    PRR_TRY(c->use_device());
+    LearnedState* L = nullptr;
+    PRR_TRY(learned_state(c, &L));
+    const int wq = (d.w + 1) / 2, hq = (d.h + 1) / 2;
+    const size_t plane = size_t(wq) * hq;
+    const int tiles_x = (d.w + kDevelopTile - 1) / kDevelopTile, tiles_y = (d.h + kDevelopTile - 1) / kDevelopTile;
+    const size_t ntiles = size_t(tiles_x) * tiles_y;
+    // Scratch: input chunks, colours, two activation buffers, head, mask.
+    const size_t o_in = 0, o_base = o_in + up256(plane * 32), o_a0 = o_base + up256(plane * 12),
+                 o_a1 = o_a0 + up256(plane * 64), o_head = o_a1 + up256(plane * 64),
+                 o_mask = o_head + up256(plane * 64), total = o_mask + up256(ntiles);
+    PRR_TRY(c->cuda(L->scratch.ensure(total)));
+    PRR_TRY(c->cuda(L->packed.ensure(sg::kPacked)));
+    PRR_TRY(c->cuda(L->counters.ensure(2)));
+    PRR_TRY(c->cuda(L->hcounters.ensure(2)));
+    uint8_t* S = L->scratch.p;
+    sg::NetBuffers nb;
+    nb.in = reinterpret_cast<uint4*>(S + o_in);
+    float* base = reinterpret_cast<float*>(S + o_base);
+    uint4* a0 = reinterpret_cast<uint4*>(S + o_a0);
+    uint4* a1 = reinterpret_cast<uint4*>(S + o_a1);
+    for (int l = 0; l < 6; l++) nb.act[l] = (l & 1) ? a1 : a0;
+    nb.head = reinterpret_cast<float*>(S + o_head);
+    uint8_t* mask = S + o_mask;
+    cudaStream_t s = c->stream;
+    PRR_TRY(c->cuda(cudaMemsetAsync(L->counters.p, 0, 2 * sizeof(unsigned), s)));
+    PRR_TRY(pack_frame(c, d, nb.in, base, nullptr));
+    PRR_TRY(c->cuda(sg::pack_weights(model->dev_params, L->packed.p, s)));
+    PRR_TRY(c->cuda(sg::forward(nb, L->packed.p, model->dev_params, nullptr, 1, hq, wq, L->counters.p + 1, s)));
+    sg::k_sg_fallback<<<unsigned(ntiles), 256, 0, s>>>(nb.in, wq, hq, tiles_x, model->noise_lo, model->noise_hi, mask,
+                                                       L->counters.p);
+    count_launch();
+    sg::OutArgs o{};
+    o.head = nb.head;
+    o.base = base;
+    o.w = d.w;
+    o.h = d.h;
+    o.wq = wq;
+    o.hq = hq;
+    o.has_matrix = d.has_matrix;
+    for (int i = 0; i < 9; i++) o.m[i] = d.m[i];
+    o.layout = layout;
+    o.r = r;
+    o.g = g;
+    o.b = b;
+    o.fallback = mask;
+    o.tiles_x = tiles_x;
+    sg::k_sg_output<<<dim3((d.w + 255) / 256, d.h), 256, 0, s>>>(o);
+    count_launch();
+    PRR_TRY(c->cuda(cudaGetLastError()));
+    // The plain develop on the fallback tiles (the others return at once).
+    d.tile_mask = mask;
+    PRR_TRY(c->cuda(launch_develop(d, s)));
+    if (fallback_tiles) {
+        PRR_TRY(c->cuda(cudaMemcpyAsync(L->hcounters.p, L->counters.p, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s)));
+        PRR_TRY(c->cuda(cudaStreamSynchronize(s)));
+        *fallback_tiles = L->hcounters.p[0];
+        if (L->hcounters.p[1]) return PRR_ERR_TIMEOUT;
+    }
+    return PRR_OK;
+}
+
+int prr_sg_trainer_create(prr_ctx* c, uint32_t batch, uint32_t crop, prr_sg_trainer** out) {
+    if (!c || !out || batch == 0 || crop < 32 || (crop & 1)) return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    prr_sg_trainer* t = new prr_sg_trainer;
+    t->ctx = c;
+    t->batch = batch;
+    t->crop = crop;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&t->sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t wq = crop / 2 + 2 * t->margin, plane = wq * wq;
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    ok(t->params.ensure(sg::kParams));
+    ok(t->grad.ensure(sg::kParams));
+    ok(t->m.ensure(sg::kParams));
+    ok(t->v.ensure(sg::kParams));
+    ok(t->packed.ensure(sg::kPacked));
+    ok(t->win_in.ensure(batch * 2 * plane));
+    ok(t->acts.ensure(6 * batch * 4 * plane));
+    ok(t->base.ensure(batch * 3 * plane));
+    ok(t->target.ensure(size_t(batch) * 3 * crop * crop));
+    ok(t->head.ensure(batch * 16 * plane));
+    ok(t->dhead.ensure(batch * 16 * plane));
+    ok(t->d0.ensure(batch * 32 * plane));
+    ok(t->d1.ensure(batch * 32 * plane));
+    ok(t->valid.ensure(batch));
+    ok(t->items.ensure(batch));
+    ok(t->hitems.ensure(batch));
+    ok(t->loss.ensure(1));
+    ok(t->hloss.ensure(1));
+    ok(t->error.ensure(1));
+    ok(t->herror.ensure(1));
+    ok(t->minmax.ensure(2));
+    ok(t->hminmax.ensure(2));
+    if (e == cudaSuccess) e = cudaMemset(t->m.p, 0, sg::kParams * 4);
+    if (e == cudaSuccess) e = cudaMemset(t->v.p, 0, sg::kParams * 4);
+    if (e == cudaSuccess) e = cudaMemset(t->params.p, 0, sg::kParams * 4);
+    if (e == cudaSuccess) e = cudaMemset(t->error.p, 0, 4);
+    if (e != cudaSuccess) {
+        prr_sg_trainer_destroy(t);
+        return c->cuda(e);
+    }
+    *out = t;
+    return PRR_OK;
+}
+
+void prr_sg_trainer_destroy(prr_sg_trainer* t) {
+    if (!t) return;
+    cudaSetDevice(t->ctx->device);
+    cudaStreamSynchronize(t->ctx->stream);
+    for (auto* f : t->frames) {
+        f->in.release();
+        f->base.release();
+        f->target.release();
+        delete f;
+    }
+    t->params.release();
+    t->grad.release();
+    t->m.release();
+    t->v.release();
+    t->minmax.release();
+    t->packed.release();
+    t->win_in.release();
+    t->acts.release();
+    t->base.release();
+    t->target.release();
+    t->head.release();
+    t->dhead.release();
+    t->d0.release();
+    t->d1.release();
+    t->valid.release();
+    t->items.release();
+    t->hitems.release();
+    t->loss.release();
+    t->hloss.release();
+    t->error.release();
+    t->herror.release();
+    t->hminmax.release();
+    delete t;
+}
+
+int prr_sg_trainer_add_frame(prr_sg_trainer* t, const prr_header* h, const prr_params* params,
+                             const uint16_t* dev_samples, uint32_t* index) {
+    if (!t || !h || !params || !dev_samples) return PRR_ERR_INVALID;
+    prr_ctx* c = t->ctx;
+    PRR_TRY(c->use_device());
+    if (h->width < t->crop || h->height < t->crop) return PRR_ERR_INVALID;
+    auto* f = new prr_sg_trainer::Frame;
+    f->w = h->width;
+    f->h = h->height;
+    f->wq = (f->w + 1) / 2;
+    f->hq = (f->h + 1) / 2;
+    const size_t plane = size_t(f->wq) * f->hq, n = size_t(f->w) * f->h;
+    cudaError_t e = f->in.ensure(2 * plane);
+    if (e == cudaSuccess) e = f->base.ensure(3 * plane);
+    if (e == cudaSuccess) e = f->target.ensure(3 * n);
+    if (e != cudaSuccess) {
+        delete f;
+        return c->cuda(e);
+    }
+    t->frames.push_back(f);
+    // The target: the plain develop, white-balanced stage, planar.
+    DevelopDesc d{};
+    PRR_TRY(build_develop_desc(h, params, PRR_STAGE_WHITE_BALANCED, dev_samples, PRR_PLANAR, f->target.p,
+                               f->target.p + n, f->target.p + 2 * n, n, &d));
+    PRR_TRY(c->cuda(launch_develop(d, c->stream)));
+    const float init[2] = {__builtin_huge_valf(), 0.0f};
+    PRR_TRY(c->cuda(cudaMemcpyAsync(t->minmax.p, init, sizeof(init), cudaMemcpyHostToDevice, c->stream)));
+    PRR_TRY(pack_frame(c, d, f->in.p, f->base.p, t->minmax.p));
+    PRR_TRY(c->cuda(cudaMemcpyAsync(t->hminmax.p, t->minmax.p, 2 * sizeof(float), cudaMemcpyDeviceToHost, c->stream)));
+    PRR_TRY(c->cuda(cudaStreamSynchronize(c->stream)));
+    const float lo = t->hminmax.p[0], hi = t->hminmax.p[1];
+    t->noise_lo = t->have_range ? std::min(t->noise_lo, lo) : lo;
+    t->noise_hi = t->have_range ? std::max(t->noise_hi, hi) : hi;
+    t->have_range = true;
+    if (index) *index = uint32_t(t->frames.size() - 1);
+    return PRR_OK;
+}
+
+int prr_sg_trainer_noise_range(prr_sg_trainer* t, float* lo, float* hi) {
+    if (!t || !lo || !hi || !t->have_range) return PRR_ERR_INVALID;
+    *lo = t->noise_lo;
+    *hi = t->noise_hi;
+    return PRR_OK;
+}
+
+int prr_sg_trainer_set_params(prr_sg_trainer* t, const float* host_params) {
+    if (!t || !host_params) return PRR_ERR_INVALID;
+    prr_ctx* c = t->ctx;
+    PRR_TRY(c->use_device());
+    PRR_TRY(c->cuda(cudaMemcpy(t->params.p, host_params, sg::kParams * 4, cudaMemcpyHostToDevice)));
+    PRR_TRY(c->cuda(cudaMemset(t->m.p, 0, sg::kParams * 4)));
+    PRR_TRY(c->cuda(cudaMemset(t->v.p, 0, sg::kParams * 4)));
+    t->step = 0;
+    return PRR_OK;
+}
+
+int prr_sg_trainer_get_params(prr_sg_trainer* t, float* host_params) {
+    if (!t || !host_params) return PRR_ERR_INVALID;
+    prr_ctx* c = t->ctx;
+    PRR_TRY(c->use_device());
+    PRR_TRY(c->cuda(cudaStreamSynchronize(c->stream)));
+    return c->cuda(cudaMemcpy(host_params, t->params.p, sg::kParams * 4, cudaMemcpyDeviceToHost));
+}
+
+const float* prr_sg_trainer_device_params(prr_sg_trainer* t) { return t ? t->params.p : nullptr; }
+
+int prr_sg_trainer_step(prr_sg_trainer* t, const uint32_t* crops, float lr, float* loss_out) {
+    if (!t || !crops) return PRR_ERR_INVALID;
+    prr_ctx* c = t->ctx;
+    PRR_TRY(c->use_device());
+    cudaStream_t s = c->stream;
+    const int B = int(t->batch), crop = int(t->crop), M = int(t->margin);
+    const int ww = crop / 2 + 2 * M, hw = ww;
+    const size_t plane = size_t(ww) * hw;
+    // The host items array is read by the copy below: wait for the last one.
+    PRR_TRY(c->cuda(cudaStreamSynchronize(s)));
+    for (int k = 0; k < B; k++) {
+        const uint32_t fi = crops[3 * k], cx = crops[3 * k + 1], cy = crops[3 * k + 2];
+        if (fi >= t->frames.size()) return PRR_ERR_INVALID;
+        const auto* f = t->frames[fi];
+        if ((cx & 1) || (cy & 1) || cx + uint32_t(crop) > uint32_t(f->w) || cy + uint32_t(crop) > uint32_t(f->h))
+            return PRR_ERR_INVALID;
+        sg::GatherItem& it = t->hitems.p[k];
+        it.in = f->in.p;
+        it.base = f->base.p;
+        it.target = f->target.p;
+        it.w = f->w;
+        it.h = f->h;
+        it.wq = f->wq;
+        it.hq = f->hq;
+        it.cx = int(cx);
+        it.cy = int(cy);
+    }
+    PRR_TRY(c->cuda(cudaMemcpyAsync(t->items.p, t->hitems.p, B * sizeof(sg::GatherItem), cudaMemcpyHostToDevice, s)));
+    sg::k_sg_gather<<<dim3((ww + 127) / 128, hw, B), 128, 0, s>>>(t->items.p, hw, ww, M, crop, t->win_in.p, t->base.p,
+                                                                   t->target.p, t->valid.p);
+    count_launch();
+    sg::NetBuffers nb;
+    nb.in = t->win_in.p;
+    for (int l = 0; l < 6; l++) nb.act[l] = t->acts.p + size_t(l) * B * 4 * plane;
+    nb.head = t->head.p;
+    PRR_TRY(c->cuda(sg::pack_weights(t->params.p, t->packed.p, s)));
+    PRR_TRY(c->cuda(sg::forward(nb, t->packed.p, t->params.p, t->valid.p, B, hw, ww, t->error.p, s)));
+    PRR_TRY(c->cuda(cudaMemsetAsync(t->dhead.p, 0, size_t(B) * 16 * plane * 4, s)));
+    PRR_TRY(c->cuda(cudaMemsetAsync(t->loss.p, 0, sizeof(double), s)));
+    const float scale = float(1.0 / (3.0 * B * double(crop) * crop));
+    sg::k_sg_loss<<<dim3((crop + 127) / 128, crop, B), 128, 0, s>>>(t->head.p, t->base.p, t->target.p, hw, ww, M, crop,
+                                                                     crop, scale, t->dhead.p, t->loss.p);
+    count_launch();
+    PRR_TRY(c->cuda(sg::backward(nb, t->params.p, t->dhead.p, t->grad.p, t->d0.p, t->d1.p, B, hw, ww, t->sms, s)));
+    t->step++;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const double bc1 = 1.0 - std::pow(double(b1), double(t->step)), bc2 = 1.0 - std::pow(double(b2), double(t->step));
+    const float lr_t = float(lr * std::sqrt(bc2) / bc1);
+    sg::k_sg_adam<<<unsigned((sg::kParams + 255) / 256), 256, 0, s>>>(t->params.p, t->grad.p, t->m.p, t->v.p, sg::kParams,
+                                                                      lr_t, b1, b2, eps);
+    count_launch();
+    PRR_TRY(c->cuda(cudaGetLastError()));
+    if (loss_out) {
+        PRR_TRY(c->cuda(cudaMemcpyAsync(t->hloss.p, t->loss.p, sizeof(double), cudaMemcpyDeviceToHost, s)));
+        PRR_TRY(c->cuda(cudaMemcpyAsync(t->herror.p, t->error.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s)));
+        PRR_TRY(c->cuda(cudaStreamSynchronize(s)));
+        *loss_out = float(t->hloss.p[0] / (3.0 * B * double(crop) * crop));
+        if (t->herror.p[0]) return PRR_ERR_TIMEOUT;
+    }
+    return PRR_OK;
+}
+
+int prr_sg_gradients(prr_ctx* c, const float* in16, const float* base3, const float* target3, uint32_t hq, uint32_t wq,
+                     const float* params, float* head_out, float* dparams, double* loss_out) {
+    if (!c || !in16 || !base3 || !target3 || !params || hq == 0 || wq == 0) return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    cudaStream_t s = c->stream;
+    const size_t plane = size_t(hq) * wq;
+    const int w = int(2 * wq), h = int(2 * hq);
+    DevBuf<float> fin, fbase, ftarget, fparams, fhead, fdhead, fgrad, d0, d1, fplanar;
+    DevBuf<uint4> in, acts;
+    DevBuf<uint16_t> packed;
+    DevBuf<double> loss;
+    DevBuf<unsigned> err;
+    auto cleanup = [&]() {
+        fin.release(); fbase.release(); ftarget.release(); fparams.release(); fhead.release(); fdhead.release();
+        fgrad.release(); d0.release(); d1.release(); fplanar.release(); in.release(); acts.release();
+        packed.release(); loss.release(); err.release();
+    };
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    ok(fplanar.ensure(16 * plane));
+    ok(fbase.ensure(3 * plane));
+    ok(ftarget.ensure(3 * size_t(w) * h));
+    ok(fparams.ensure(sg::kParams));
+    ok(fhead.ensure(16 * plane));
+    ok(fdhead.ensure(16 * plane));
+    ok(fgrad.ensure(sg::kParams));
+    ok(d0.ensure(32 * plane));
+    ok(d1.ensure(32 * plane));
+    ok(in.ensure(2 * plane));
+    ok(acts.ensure(6 * 4 * plane));
+    ok(packed.ensure(sg::kPacked));
+    ok(loss.ensure(1));
+    ok(err.ensure(1));
+    ok(cudaMemcpyAsync(fplanar.p, in16, 16 * plane * 4, cudaMemcpyHostToDevice, s));
+    ok(cudaMemcpyAsync(fbase.p, base3, 3 * plane * 4, cudaMemcpyHostToDevice, s));
+    ok(cudaMemcpyAsync(ftarget.p, target3, 3 * size_t(w) * h * 4, cudaMemcpyHostToDevice, s));
+    ok(cudaMemcpyAsync(fparams.p, params, sg::kParams * 4, cudaMemcpyHostToDevice, s));
+    ok(cudaMemsetAsync(fdhead.p, 0, 16 * plane * 4, s));
+    ok(cudaMemsetAsync(loss.p, 0, 8, s));
+    ok(cudaMemsetAsync(err.p, 0, 4, s));
+    if (e != cudaSuccess) {
+        cleanup();
+        return c->cuda(e);
+    }
+    sg::k_sg_from_planar<<<unsigned((plane + 127) / 128), 128, 0, s>>>(fplanar.p, int(plane), in.p);
+    count_launch();
+    sg::NetBuffers nb;
+    nb.in = in.p;
+    for (int l = 0; l < 6; l++) nb.act[l] = acts.p + size_t(l) * 4 * plane;
+    nb.head = fhead.p;
+    ok(sg::pack_weights(fparams.p, packed.p, s));
+    ok(sg::forward(nb, packed.p, fparams.p, nullptr, 1, int(hq), int(wq), err.p, s));
+    const float scale = float(1.0 / (3.0 * double(w) * h));
+    sg::k_sg_loss<<<dim3((w + 127) / 128, h, 1), 128, 0, s>>>(fhead.p, fbase.p, ftarget.p, int(hq), int(wq), 0, w, h,
+                                                               scale, fdhead.p, loss.p);
+    count_launch();
+    int sms = 148;
+    ok(sg::backward(nb, fparams.p, fdhead.p, fgrad.p, d0.p, d1.p, 1, int(hq), int(wq), sms, s));
+    double hl = 0.0;
+    unsigned he = 0;
+    if (head_out) ok(cudaMemcpyAsync(head_out, fhead.p, 16 * plane * 4, cudaMemcpyDeviceToHost, s));
+    if (dparams) ok(cudaMemcpyAsync(dparams, fgrad.p, sg::kParams * 4, cudaMemcpyDeviceToHost, s));
+    ok(cudaMemcpyAsync(&hl, loss.p, 8, cudaMemcpyDeviceToHost, s));
+    ok(cudaMemcpyAsync(&he, err.p, 4, cudaMemcpyDeviceToHost, s));
+    ok(cudaStreamSynchronize(s));
+    cleanup();
+    if (e != cudaSuccess) return c->cuda(e);
+    if (loss_out) *loss_out = hl / (3.0 * double(w) * h);
+    return he ? PRR_ERR_TIMEOUT : PRR_OK;
+}
+
+}  // extern "C"

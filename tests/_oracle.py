@@ -136,6 +136,14 @@ def lib():
         L.orc_green_pass.argtypes = [vp, sz, sz, C.POINTER(Params), vp]
         L.orc_chroma_pass.argtypes = [vp, sz, sz, C.POINTER(Params), vp]
         L.orc_apply_matrix.argtypes = [vp, sz, vp, vp]
+        L.orc_sg_param_count.restype = sz
+        L.orc_sg_pack.restype = C.c_int
+        L.orc_sg_pack.argtypes = [C.POINTER(Header), vp, C.POINTER(Params), vp, vp]
+        L.orc_sg_forward.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int, vp, vp]
+        L.orc_sg_output.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
+        L.orc_sg_loss.restype = C.c_double
+        L.orc_sg_loss.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
+        L.orc_sg_backward.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -352,3 +360,57 @@ def apply_matrix(rgb: np.ndarray, m: np.ndarray) -> np.ndarray:
     out = np.zeros_like(x)
     lib().orc_apply_matrix(_p(x), x.size // 3, _p(mm), _p(out))
     return out
+
+
+# --- learned demosaic surrogate (sg_oracle.h) ------------------------------------
+
+
+def sg_param_count() -> int:
+    return int(lib().orc_sg_param_count())
+
+
+def sg_pack(h: Header, samples: np.ndarray, p: Params):
+    wq, hq = (h.width + 1) // 2, (h.height + 1) // 2
+    in16 = np.zeros((16, hq, wq), dtype=np.float32)
+    base = np.zeros((3, hq, wq), dtype=np.float32)
+    s = np.ascontiguousarray(samples, dtype=np.uint16)
+    assert lib().orc_sg_pack(C.byref(h), _p(s), C.byref(p), _p(in16), _p(base)) == 0
+    return in16, base
+
+
+def sg_forward(in16: np.ndarray, params: np.ndarray, round_bf16: bool = True):
+    _, hq, wq = in16.shape
+    acts = np.zeros((6, 32, hq, wq), dtype=np.float32)
+    head = np.zeros((16, hq, wq), dtype=np.float32)
+    a = np.ascontiguousarray(in16, dtype=np.float32)
+    pr = np.ascontiguousarray(params, dtype=np.float32)
+    lib().orc_sg_forward(_p(a), hq, wq, _p(pr), 1 if round_bf16 else 0, _p(acts), _p(head))
+    return acts, head
+
+
+def sg_output(head, base, width, height, m9=None):
+    _, hq, wq = head.shape
+    out = np.zeros((3, height, width), dtype=np.float32)
+    m = None if m9 is None else np.ascontiguousarray(m9, dtype=np.float32)
+    lib().orc_sg_output(_p(np.ascontiguousarray(head)), _p(np.ascontiguousarray(base)), hq, wq, width, height,
+                        None if m is None else _p(m), _p(out[0]), _p(out[1]), _p(out[2]))
+    return out
+
+
+def sg_loss(head, base, target):
+    _, hq, wq = head.shape
+    _, height, width = target.shape
+    dhead = np.zeros_like(head)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    loss = lib().orc_sg_loss(_p(np.ascontiguousarray(head)), _p(np.ascontiguousarray(base)), hq, wq, width,
+                             height, _p(t[0]), _p(t[1]), _p(t[2]), _p(dhead))
+    return float(loss), dhead
+
+
+def sg_backward(in16, params, acts, dhead):
+    _, hq, wq = in16.shape
+    dp = np.zeros(sg_param_count(), dtype=np.float32)
+    lib().orc_sg_backward(_p(np.ascontiguousarray(in16, dtype=np.float32)), hq, wq,
+                          _p(np.ascontiguousarray(params, dtype=np.float32)), _p(np.ascontiguousarray(acts)),
+                          _p(np.ascontiguousarray(dhead)), _p(dp))
+    return dp
