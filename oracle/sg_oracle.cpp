@@ -89,16 +89,21 @@ int orc_sg_pack(const orc_header* hdr, const uint16_t* samples, const orc_params
         const float gb = nrm(2 * i + rc, 2 * j + 1 - rr);
         return (gr + gb) * 0.5f;
     };
+    // Network quad (i, j) is picture quad (si, sj): mirrored by the red
+    // sensel's column and row, so that every pattern is seen as RGGB.
+    const int ex = rc ? -1 : 1, sy = rr ? -1 : 1;
     for (int j = 0; j < hq; j++)
         for (int i = 0; i < wq; i++) {
-            const int x0 = 2 * i, y0 = 2 * j;
+            const int si = rc ? wq - 1 - i : i, sj = rr ? hq - 1 - j : j;
+            const int x0 = 2 * si, y0 = 2 * sj;
             const float r = nrm(x0 + rc, y0 + rr) * p->wb[0];
             const float gr = nrm(x0 + 1 - rc, y0 + rr);
             const float gb = nrm(x0 + rc, y0 + 1 - rr);
             const float b = nrm(x0 + 1 - rc, y0 + 1 - rr) * p->wb[1];
             const float gm = (gr + gb) * 0.5f;
             const float noise = 64.0f * std::sqrt(variance(gm, bs, p->noise));
-            const float ge = green(i + 1, j), gw = green(i - 1, j), gs = green(i, j + 1), gn = green(i, j - 1);
+            const float ge = green(si + ex, sj), gw = green(si - ex, sj), gs = green(si, sj + sy),
+                        gn = green(si, sj - sy);
             const float gx = (ge - gw) * 0.5f, gy = (gs - gn) * 0.5f;
             const float lap = gm - ((ge + gw) + (gs + gn)) * 0.25f;
             const size_t q = size_t(j) * wq + i;
@@ -135,13 +140,15 @@ void orc_sg_forward(const float* in16, int h, int w, const float* params, int ro
     }
 }
 
-void orc_sg_output(const float* head, const float* base3, int hq, int wq, int width, int height,
+void orc_sg_output(const float* head, const float* base3, int hq, int wq, int width, int height, int cfa,
                    const float* m9, float* r, float* g, float* b) {
     const size_t plane = size_t(hq) * wq;
+    const int rr = cfa >> 1, rc = cfa & 1;
     for (int y = 0; y < height; y++)
         for (int x = 0; x < width; x++) {
-            const size_t q = size_t(y >> 1) * wq + (x >> 1);
-            const int s = (y & 1) * 2 + (x & 1);
+            const int qi = rc ? wq - 1 - (x >> 1) : (x >> 1), qj = rr ? hq - 1 - (y >> 1) : (y >> 1);
+            const size_t q = size_t(qj) * wq + qi;
+            const int s = ((y & 1) ^ rr) * 2 + ((x & 1) ^ rc);
             float rv = std::min(head[(0 + s) * plane + q] + base3[q], 1.0f);
             float gv = std::min(head[(4 + s) * plane + q] + base3[plane + q], 1.0f);
             float bv = std::min(head[(8 + s) * plane + q] + base3[2 * plane + q], 1.0f);

@@ -21,10 +21,15 @@
  *          stored as bf16; head conv 3x3 32->16 (12 used) + bias, f32.
  *          Zero padding outside the image at every layer; products of bf16
  *          values accumulated in f32;
- *  output  full-resolution RGB: head channel c*4 + 2*sy + sx of quad (i, j)
- *          plus the quad's own colour (red, mean green, blue) gives pixel
- *          (2i + sx, 2j + sy); min(., 1) and the Rec.2020 matrix for that
- *          stage, as the plain develop applies them.
+ *  frame   the network works on the picture mirrored horizontally when red
+ *          sits in the right column of a quad and vertically when it sits in
+ *          the bottom row, so every Bayer pattern reaches it as RGGB;
+ *  output  full-resolution RGB: head channel c*4 + 2*sy + sx of network quad
+ *          (i, j) plus the quad's own colour (red, mean green, blue) gives
+ *          network pixel (2i + sx, 2j + sy), mirrored back to the picture;
+ *          min(., 1) and the Rec.2020 matrix for that stage, as the plain
+ *          develop applies them. The loss and its gradient are stated in the
+ *          network frame (targets mirrored into it).
  *
  * Parameters are f32, layer by layer: weights [cout][cin][9] (tap = 3*dy +
  * dx), then bias [cout].
@@ -55,8 +60,9 @@ void orc_sg_forward(const float* in16, int h, int w, const float* params, int ro
                     float* head);
 
 /* Full-resolution RGB from head and base (planar, width x height visible
- * pixels); m9 NULL for the white-balanced stage. */
-void orc_sg_output(const float* head, const float* base3, int hq, int wq, int width, int height,
+ * pixels, mirrored back from the network frame of Bayer phase `cfa`); m9
+ * NULL for the white-balanced stage. */
+void orc_sg_output(const float* head, const float* base3, int hq, int wq, int width, int height, int cfa,
                    const float* m9, float* r, float* g, float* b);
 
 /* Mean squared error of the unclipped output against target planes over the

@@ -17,8 +17,12 @@
 //  layers  conv 3x3 16->32, five conv 3x3 32->32 (bias, ReLU, bf16), head
 //          conv 3x3 32->16 (12 used; bias, f32); zero padding at every layer;
 //          bf16 products accumulated in f32 (tcgen05.mma kind::f16);
-//  output  head channel c*4 + 2*sy + sx of a quad plus the quad's colour
-//          (red, mean green, blue) is pixel (2i + sx, 2j + sy); min(., 1), then
+//  frame   the network sees the picture mirrored horizontally when red sits
+//          in the right column of a quad and vertically when it sits in the
+//          bottom row: every Bayer pattern reaches it as RGGB;
+//  output  head channel c*4 + 2*sy + sx of a network-frame quad plus the
+//          quad's colour (red, mean green, blue) is network pixel
+//          (2i + sx, 2j + sy), mirrored back to the picture; min(., 1), then
 //          the Rec.2020 matrix for that stage.
 //
 // Data layouts: activations bf16 in channel chunks, [image][C/8][H][W][8]
@@ -166,6 +170,13 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint64
     return false;
 }
 
+// 16-byte global -> shared copy without a register round trip; `full`
+// false writes 16 zero bytes (nothing is read).
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool full) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(full ? 16 : 0)
+                 : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -221,17 +232,21 @@ __global__ void __launch_bounds__(kConvThreads) k_sg_conv(ConvArgs a) {
     uint8_t* win = smem;
     uint8_t* wsm = smem + C::WIN_BYTES;
 
-    // Window (zero outside the image) and weights, 16 bytes per access.
+    // Window (zero outside the image) and weights: 16-byte asynchronous
+    // copies, all in flight at once (a source size of 0 fills zeros).
     const uint4* xb = a.x + size_t(img) * C::C8 * a.H * a.W;
+    const uint32_t win_s = smem_u32(win), wsm_s = smem_u32(wsm);
     for (int v = tid; v < C::C8 * WY * WX; v += kConvThreads) {
         const int c = v / (WY * WX), r = (v / WX) % WY, q = v % WX;
         const int gy = ty0 - 1 + r, gx = tx0 - 1 + q;
-        uint4 val = make_uint4(0, 0, 0, 0);
-        if (gy >= 0 && gy < a.H && gx >= 0 && gx < a.W) val = __ldg(xb + (size_t(c) * a.H + gy) * a.W + gx);
-        *reinterpret_cast<uint4*>(win + c * C::CS + r * C::RP + q * 16) = val;
+        const bool in = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
+        const uint4* src = in ? xb + (size_t(c) * a.H + gy) * a.W + gx : xb;
+        cp_async16(win_s + uint32_t(c * C::CS + r * C::RP + q * 16), src, in);
     }
-    for (int v = tid; v < C::W_BYTES / 16; v += kConvThreads) reinterpret_cast<uint4*>(wsm)[v] = __ldg(a.w + v);
-    // Generic-proxy stores become visible to the tensor core's reads.
+    for (int v = tid; v < C::W_BYTES / 16; v += kConvThreads) cp_async16(wsm_s + uint32_t(v * 16), a.w + v, true);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // The copies become visible to the tensor core's reads (async proxy).
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -338,7 +353,7 @@ struct PackArgs {
     uint32_t stride;
     int w, h, wq, hq;
     uint32_t c0[8], cd[8];
-    int rr, rc, black;
+    int rr, rc, black;  // red sensel of a quad (row, column); the network frame mirrors by them
     float one_over_range, bs, wb0, wb1;
     float n0, n1, n2;
     uint4* in;      // [2][hq][wq] chunks
@@ -362,11 +377,18 @@ __device__ __forceinline__ float sg_green(const PackArgs& p, int i, int j) {
     return __fmul_rn(__fadd_rn(gr, gb), 0.5f);
 }
 
+// Network-frame quad (i, j) is picture quad (i, j) mirrored horizontally
+// when red sits in the right column of a quad and vertically when it sits in
+// the bottom row, so that every Bayer pattern reaches the network as RGGB.
+__host__ __device__ __forceinline__ int mirror_q(int i, int n, int flip) { return flip ? n - 1 - i : i; }
+
 __global__ void k_sg_pack(PackArgs p) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= p.wq) return;
-    const int x0 = 2 * i, y0 = 2 * j;
+    const int si = mirror_q(i, p.wq, p.rc), sj = mirror_q(j, p.hq, p.rr);  // picture quad
+    const int ex = p.rc ? -1 : 1, sy = p.rr ? -1 : 1;                     // network east / south
+    const int x0 = 2 * si, y0 = 2 * sj;
     const float r = __fmul_rn(sg_nrm(p, x0 + p.rc, y0 + p.rr), p.wb0);
     const float gr = sg_nrm(p, x0 + 1 - p.rc, y0 + p.rr);
     const float gb = sg_nrm(p, x0 + p.rc, y0 + 1 - p.rr);
@@ -375,8 +397,8 @@ __global__ void k_sg_pack(PackArgs p) {
     const float t = __fadd_rn(p.bs, gm);
     const float var = __fadd_rn(p.n2, fmaxf(p.n1, __fmul_rn(p.n0, __fmul_rn(t, t))));
     const float noise = __fmul_rn(64.0f, __fsqrt_rn(var));
-    const float ge = sg_green(p, i + 1, j), gw = sg_green(p, i - 1, j);
-    const float gs = sg_green(p, i, j + 1), gn = sg_green(p, i, j - 1);
+    const float ge = sg_green(p, si + ex, sj), gw = sg_green(p, si - ex, sj);
+    const float gs = sg_green(p, si, sj + sy), gn = sg_green(p, si, sj - sy);
     const float gx = __fmul_rn(__fsub_rn(ge, gw), 0.5f), gy = __fmul_rn(__fsub_rn(gs, gn), 0.5f);
     const float lap = __fsub_rn(gm, __fmul_rn(__fadd_rn(__fadd_rn(ge, gw), __fadd_rn(gs, gn)), 0.25f));
     auto d4 = [](float v, float ref) { return __fmul_rn(__fsub_rn(v, ref), 4.0f); };
@@ -412,9 +434,10 @@ __global__ void k_sg_pack_weights(const float* __restrict__ params, uint16_t* __
 }
 
 struct OutArgs {
-    const float* head;  // [16][hq][wq]
-    const float* base;  // [3][hq][wq]
+    const float* head;  // [16][hq][wq], network frame
+    const float* base;  // [3][hq][wq], network frame
     int w, h, wq, hq;
+    int rr, rc;         // mirrors of the network frame
     int has_matrix;
     float m[9];
     int layout;
@@ -430,8 +453,8 @@ __global__ void k_sg_output(OutArgs o) {
     if (x >= o.w) return;
     if (o.fallback && o.fallback[(y / kDevelopTile) * o.tiles_x + x / kDevelopTile]) return;
     const size_t plane = size_t(o.wq) * o.hq;
-    const size_t q = size_t(y >> 1) * o.wq + (x >> 1);
-    const int s = (y & 1) * 2 + (x & 1);
+    const size_t q = size_t(mirror_q(y >> 1, o.hq, o.rr)) * o.wq + mirror_q(x >> 1, o.wq, o.rc);
+    const int s = ((y & 1) ^ o.rr) * 2 + ((x & 1) ^ o.rc);
     float r = fminf(__fadd_rn(o.head[(0 + s) * plane + q], o.base[q]), 1.0f);
     float g = fminf(__fadd_rn(o.head[(4 + s) * plane + q], o.base[plane + q]), 1.0f);
     float b = fminf(__fadd_rn(o.head[(8 + s) * plane + q], o.base[2 * plane + q]), 1.0f);
@@ -453,15 +476,16 @@ __global__ void k_sg_output(OutArgs o) {
     }
 }
 
-// Per 32x32 output tile: does any quad's noise channel leave [lo, hi]?
-__global__ void k_sg_fallback(const uint4* __restrict__ in, int wq, int hq, int tiles_x, float lo, float hi,
-                              uint8_t* __restrict__ mask, unsigned* __restrict__ count) {
+// Per 32x32 picture tile: does any quad's noise channel leave [lo, hi]?
+__global__ void k_sg_fallback(const uint4* __restrict__ in, int wq, int hq, int rr, int rc, int tiles_x, float lo,
+                              float hi, uint8_t* __restrict__ mask, unsigned* __restrict__ count) {
     const int tile = blockIdx.x;
     const int qx0 = (tile % tiles_x) * (kDevelopTile / 2), qy0 = (tile / tiles_x) * (kDevelopTile / 2);
     const int u = threadIdx.x % 16, v = threadIdx.x / 16;
     int out = 0;
     if (qx0 + u < wq && qy0 + v < hq) {
-        const float n = bf16_lo(in[size_t(qy0 + v) * wq + qx0 + u].z);
+        const size_t q = size_t(mirror_q(qy0 + v, hq, rr)) * wq + mirror_q(qx0 + u, wq, rc);
+        const float n = bf16_lo(in[q].z);
         out = (n < lo || n > hi) ? 1 : 0;
     }
     out = __syncthreads_or(out);
@@ -474,11 +498,12 @@ __global__ void k_sg_fallback(const uint4* __restrict__ in, int wq, int hq, int 
 // --- training ------------------------------------------------------------------------
 
 struct GatherItem {
-    const uint4* in;      // frame input chunks [2][hq][wq]
-    const float* base;    // [3][hq][wq]
-    const float* target;  // plain develop, white-balanced, planar [3][h][w]
+    const uint4* in;      // frame input chunks [2][hq][wq], network frame
+    const float* base;    // [3][hq][wq], network frame
+    const float* target;  // plain develop, white-balanced, planar [3][h][w], picture frame
     int w, h, wq, hq;
-    int cx, cy;           // crop origin, full resolution, even
+    int rr, rc;           // mirrors of the network frame
+    int cx, cy;           // crop origin in the network frame, full resolution, even
 };
 
 // Window u, v of image k is frame quad (cx/2 - margin + u, cy/2 - margin + v).
@@ -505,7 +530,9 @@ __global__ void k_sg_gather(const GatherItem* __restrict__ items, int hw, int ww
         for (int dy = 0; dy < 2; dy++)
             for (int dx = 0; dx < 2; dx++) {
                 const int x = 2 * u + dx, y = 2 * v + dy;
-                const size_t fi = size_t(it.cy + y) * it.w + it.cx + x;
+                const int px = it.rc ? it.w - 1 - (it.cx + x) : it.cx + x;
+                const int py = it.rr ? it.h - 1 - (it.cy + y) : it.cy + y;
+                const size_t fi = size_t(py) * it.w + px;
                 for (int c = 0; c < 3; c++)
                     target[((size_t(k) * 3 + c) * crop + y) * crop + x] = it.target[size_t(c) * it.w * it.h + fi];
             }
@@ -789,7 +816,7 @@ struct prr_sg_trainer {
         DevBuf<uint4> in;
         DevBuf<float> base;
         DevBuf<float> target;
-        int w = 0, h = 0, wq = 0, hq = 0;
+        int w = 0, h = 0, wq = 0, hq = 0, rr = 0, rc = 0;
     };
     std::vector<Frame*> frames;
     DevBuf<float> params, grad, m, v, minmax;
@@ -895,8 +922,8 @@ int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* param
     PRR_TRY(pack_frame(c, d, nb.in, base, nullptr));
     PRR_TRY(c->cuda(sg::pack_weights(model->dev_params, L->packed.p, s)));
     PRR_TRY(c->cuda(sg::forward(nb, L->packed.p, model->dev_params, nullptr, 1, hq, wq, L->counters.p + 1, s)));
-    sg::k_sg_fallback<<<unsigned(ntiles), 256, 0, s>>>(nb.in, wq, hq, tiles_x, model->noise_lo, model->noise_hi, mask,
-                                                       L->counters.p);
+    sg::k_sg_fallback<<<unsigned(ntiles), 256, 0, s>>>(nb.in, wq, hq, d.cfa >> 1, d.cfa & 1, tiles_x, model->noise_lo,
+                                                       model->noise_hi, mask, L->counters.p);
     count_launch();
     sg::OutArgs o{};
     o.head = nb.head;
@@ -905,6 +932,8 @@ int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* param
     o.h = d.h;
     o.wq = wq;
     o.hq = hq;
+    o.rr = d.cfa >> 1;
+    o.rc = d.cfa & 1;
     o.has_matrix = d.has_matrix;
     for (int i = 0; i < 9; i++) o.m[i] = d.m[i];
     o.layout = layout;
@@ -1035,6 +1064,8 @@ int prr_sg_trainer_add_frame(prr_sg_trainer* t, const prr_header* h, const prr_p
     PRR_TRY(build_develop_desc(h, params, PRR_STAGE_WHITE_BALANCED, dev_samples, PRR_PLANAR, f->target.p,
                                f->target.p + n, f->target.p + 2 * n, n, &d));
     PRR_TRY(c->cuda(launch_develop(d, c->stream)));
+    f->rr = d.cfa >> 1;
+    f->rc = d.cfa & 1;
     const float init[2] = {__builtin_huge_valf(), 0.0f};
     PRR_TRY(c->cuda(cudaMemcpyAsync(t->minmax.p, init, sizeof(init), cudaMemcpyHostToDevice, c->stream)));
     PRR_TRY(pack_frame(c, d, f->in.p, f->base.p, t->minmax.p));
@@ -1100,6 +1131,8 @@ int prr_sg_trainer_step(prr_sg_trainer* t, const uint32_t* crops, float lr, floa
         it.h = f->h;
         it.wq = f->wq;
         it.hq = f->hq;
+        it.rr = f->rr;
+        it.rc = f->rc;
         it.cx = int(cx);
         it.cy = int(cy);
     }

@@ -140,7 +140,7 @@ def lib():
         L.orc_sg_pack.restype = C.c_int
         L.orc_sg_pack.argtypes = [C.POINTER(Header), vp, C.POINTER(Params), vp, vp]
         L.orc_sg_forward.argtypes = [vp, C.c_int, C.c_int, vp, C.c_int, vp, vp]
-        L.orc_sg_output.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
+        L.orc_sg_output.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
         L.orc_sg_loss.restype = C.c_double
         L.orc_sg_loss.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
         L.orc_sg_backward.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp]
@@ -388,11 +388,11 @@ def sg_forward(in16: np.ndarray, params: np.ndarray, round_bf16: bool = True):
     return acts, head
 
 
-def sg_output(head, base, width, height, m9=None):
+def sg_output(head, base, width, height, m9=None, cfa=0):
     _, hq, wq = head.shape
     out = np.zeros((3, height, width), dtype=np.float32)
     m = None if m9 is None else np.ascontiguousarray(m9, dtype=np.float32)
-    lib().orc_sg_output(_p(np.ascontiguousarray(head)), _p(np.ascontiguousarray(base)), hq, wq, width, height,
+    lib().orc_sg_output(_p(np.ascontiguousarray(head)), _p(np.ascontiguousarray(base)), hq, wq, width, height, cfa,
                         None if m is None else _p(m), _p(out[0]), _p(out[1]), _p(out[2]))
     return out
 

@@ -107,7 +107,7 @@ def test_network_free_output_is_exact(pattern, stage):
     _, base = O.sg_pack(of.header, of.samples, p)
     head = np.zeros((16,) + base.shape[1:], dtype=np.float32)
     m = O.output_matrix(of.header) if stage == P.Stage.REC2020 else None
-    want = O.sg_output(head, base, 200, 132, m)
+    want = O.sg_output(head, base, 200, 132, m, cfa=p.cfa_phase)
     assert np.array_equal(got.reshape(3, 132, 200), want)
 
 
@@ -127,7 +127,7 @@ def test_fallback_tiles_are_the_plain_develop():
     assert n0 == 0
     of = O.decode_frame(pkt)
     in16, _ = O.sg_pack(of.header, of.samples, O.params_new(of.header, of.quantizer))
-    noise = in16[4]
+    noise = in16[4]  # RGGB: the network frame is the picture frame
     hi = float(np.median(noise))
     mixed, n1 = planes_of(frame, P.Stage.REC2020, Lrn.Surrogate(params, 0.0, hi))
     assert 0 < n1 < 40

@@ -96,9 +96,10 @@ def test_bf16_rounding_is_round_to_nearest_even():
 def test_pack_follows_the_plain_develop_normalization():
     import proresraw_rs_b200.synth as S
 
+    # RGGB: the network frame is the picture frame.
     w, h = 36, 22
-    m = S.mosaic(w, h, S.GRBG, seed=4, sigma=12.0)
-    spec = S.Spec(w, h, pattern=S.GRBG, alignment=1, white_level=4095, valid_tiles=True, wb=(1.7, 1.3))
+    m = S.mosaic(w, h, S.RGGB, seed=4, sigma=12.0)
+    spec = S.Spec(w, h, pattern=S.RGGB, alignment=1, white_level=4095, valid_tiles=True, wb=(1.7, 1.3))
     pkt = S.encode(spec, m, qscale=20)
     f = O.decode_frame(pkt)
     p = O.params_with_white_balance(f.header, f.quantizer, 1.7, 1.3)
@@ -127,3 +128,29 @@ def test_pack_follows_the_plain_develop_normalization():
     lap = gm - ((pad[1:-1, 2:] + pad[1:-1, :-2]) + (pad[2:, 1:-1] + pad[:-2, 1:-1])) * np.float32(0.25)
     assert near(in16[6], gx * four) and near(in16[7], gy * four) and near(in16[8], lap * four)
     assert np.all(in16[4] > 0.0)
+
+
+@pytest.mark.parametrize("pattern", [1, 2, 3])
+def test_every_pattern_packs_as_rggb_in_the_network_frame(pattern):
+    # A frame and its mirror image with red moved to the top-left: the
+    # network sees the same input.
+    import proresraw_rs_b200.synth as S
+
+    w, h = 36, 22
+    m = S.mosaic(w, h, pattern, seed=9, sigma=12.0)
+    rr, rc = pattern >> 1, pattern & 1
+    flipped = m[::-1 if rr else 1, ::-1 if rc else 1].copy()
+    spec_a = S.Spec(w, h, pattern=pattern, alignment=1, white_level=4095, valid_tiles=True)
+    spec_b = S.Spec(w, h, pattern=S.RGGB, alignment=1, white_level=4095, valid_tiles=True)
+    # Lossless enough: qscale 1 keeps the codes within the transform's rounding.
+    fa = O.decode_frame(S.encode(spec_a, m, qscale=1))
+    fb = O.decode_frame(S.encode(spec_b, flipped, qscale=1))
+    sa = fa.samples.reshape(-1, (w + 15) // 16 * 16)[:h, :w]
+    sb = fb.samples.reshape(-1, (w + 15) // 16 * 16)[:h, :w]
+    fb.samples.reshape(-1, (w + 15) // 16 * 16)[:h, :w] = sa[::-1 if rr else 1, ::-1 if rc else 1]
+    pa = O.params_new(fa.header, fa.quantizer)
+    pb = O.params_new(fb.header, fb.quantizer)
+    ia, ba = O.sg_pack(fa.header, fa.samples, pa)
+    ib, bb = O.sg_pack(fb.header, fb.samples, pb)
+    assert np.array_equal(ia, ib) and np.array_equal(ba, bb)
+    assert sb.shape == sa.shape
