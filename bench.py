@@ -41,6 +41,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from proresraw_rs_b200 import replicas as R  # noqa: E402
+
 W, H = 5760, 3040
 RING = 3
 
@@ -558,19 +560,340 @@ def run_batch_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Learned develop workloads. The surrogate is trained here, on the device,
+# by the library's own kernels: 4000 random 512x512 crops of synthetic
+# 4096x2160 RGGB frames (the mosaic generator with noise sigma uniform in
+# [4, 32], qscale uniform in [15, 45]) developed by the plain GPU path, Adam
+# at lr 1e-3, batch 32. One step of the "learned" workload = one held-out
+# 4096x2160 frame developed to planar Rec.2020 by the network (device-
+# resident codes); the plain develop of the same frames is timed beside it.
+
+LEARN_W, LEARN_H = 4096, 2160
+LEARN_TRAIN_FRAMES, LEARN_HELD = 12, 16
+
+
+def learn_frame(seed, rng):
+    from proresraw_rs_b200 import synth as S
+
+    sigma, q = float(rng.uniform(4, 32)), int(rng.integers(15, 46))
+    m = S.mosaic(LEARN_W, LEARN_H, S.RGGB, seed=seed, sigma=sigma, white=4095)
+    spec = S.Spec(LEARN_W, LEARN_H, pattern=S.RGGB, alignment=2, white_level=4095, version=1, valid_tiles=True,
+                  wb=(1.9, 1.4), color_matrix=(0.61, 0.25, 0.10, 0.26, 0.89, -0.15, 0.02, -0.09, 1.17))
+    return S.encode(spec, m, qscale=q, qscale_seed=seed), sigma, q
+
+
+def sg_flops_per_frame(w, h):
+    """Algorithmic FLOPs of the network per frame: 5 input channels, six
+    32-channel 3x3 layers, a 12-channel head, per half-resolution pixel."""
+    return 2 * 9 * (5 * 32 + 5 * 32 * 32 + 32 * 12) * ((w + 1) // 2) * ((h + 1) // 2)
+
+
+def tensor_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured bf16_tflops (burst)"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def train_for_bench(P, L, epochs, log=None):
+    rng = np.random.default_rng(0)
+    frames = [P.decode_frame(learn_frame(1000 + k, rng)[0]) for k in range(LEARN_TRAIN_FRAMES)]
+    t0 = time.perf_counter()
+    s, hist = L.train_surrogate(frames, crops=4000, batch=32, crop=512, epochs=epochs, lr=1e-3, seed=0, log=log)
+    import torch
+
+    torch.cuda.synchronize()
+    return s, hist, time.perf_counter() - t0
+
+
+def run_learned(args):
+    import torch
+
+    import proresraw_rs_b200 as P
+    from proresraw_rs_b200 import learned as L
+
+    world, rank, local = dist_setup(args.gpus)
+    s, hist, train_s = train_for_bench(P, L, args.epochs)
+    rng = np.random.default_rng(4242)
+    held = [learn_frame(2000 + k, rng) for k in range(LEARN_HELD)]
+    frames = [P.decode_frame(pk) for pk, _, _ in held]
+    n = LEARN_W * LEARN_H
+    out = [torch.empty(n, dtype=torch.float32, device="cuda") for _ in range(3)]
+    dp = s.device()
+    prms = [P.DemosaicParams.new(f.header, f.quantizer()) for f in frames]
+    psnrs, maxabs, fb = [], [], 0
+    for f, prm in zip(frames, prms):
+        fb += L.develop_learned_planar_into(f, prm, P.Stage.REC2020, s, out, dev_params=dp)
+        got = np.stack([o.cpu().numpy() for o in out])
+        plain = P.develop_planar(f, prm, P.Stage.REC2020)
+        want = np.stack([p.cpu().numpy() for p in plain.planes])
+        psnrs.append(L.psnr(got, want))
+        maxabs.append(L.max_abs(got, want))
+    tiles = ((LEARN_W + 31) // 32) * ((LEARN_H + 31) // 32) * len(frames)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, steps):
+        for k in range(max(3, args.warmup)):
+            fn(k)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(steps):
+            fn(k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def learned_step(k):
+        f = frames[k % len(frames)]
+        L.develop_learned_planar_into(f, prms[k % len(frames)], P.Stage.REC2020, s, out, dev_params=dp,
+                                      count_fallback=False)
+
+    def plain_step(k):
+        f = frames[k % len(frames)]
+        P.develop_planar_into(f, prms[k % len(frames)], P.Stage.REC2020, out)
+
+    launches0 = P.kernel_launches()
+    with Clocks(torch.cuda.current_device()) as clocks:
+        ms_learned = timed(learned_step, args.steps)
+    launches = P.kernel_launches() - launches0
+    ms_plain = timed(plain_step, args.steps)
+    ms_l, ms_p = R.reduce_max(ms_learned), R.reduce_max(ms_plain)
+    # End to end: host packet in, decode, learned develop, planes to pinned host memory.
+    host = torch.empty(3 * n, dtype=torch.float32, pin_memory=True)
+
+    def e2e_step(k):
+        f = P.decode_frame(held[k % len(held)][0])
+        L.develop_learned_planar_into(f, prms[k % len(frames)], P.Stage.REC2020, s, out, dev_params=dp)
+        for c in range(3):
+            host[c * n:(c + 1) * n].copy_(out[c], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for k in range(2):
+        e2e_step(k)
+    t0 = time.perf_counter()
+    e2e_n = max(4, args.steps // 4)
+    for k in range(e2e_n):
+        e2e_step(k)
+    e2e_s = R.reduce_max(time.perf_counter() - t0)
+    if rank == 0:
+        peak, pk = tensor_peak()
+        flops = sg_flops_per_frame(LEARN_W, LEARN_H)
+        line = {
+            "metric": "learned develop frames/s (4096x2160 to planar Rec.2020)", "value": world * 1000.0 / ms_l,
+            "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_l,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (f32 accumulate)",
+            "data": "synthetic",
+            "config": {"workload": "surrogate develop of 16 held-out 4096x2160 RGGB frames (sigma U[4,32], qscale "
+                                   "U[15,45]); trained on 4000 512x512 crops, batch 32, Adam lr 1e-3",
+                       "train_epochs": args.epochs, "train_seconds": train_s,
+                       "train_loss_first_last": [hist[0], hist[-1]],
+                       "plain_develop_ms": ms_p, "plain_develop_frames_per_s": 1000.0 / ms_p,
+                       "learned_over_plain_speed": ms_p / ms_l,
+                       "psnr_db_vs_plain": {"min": min(psnrs), "mean": float(np.mean(psnrs)), "max": max(psnrs)},
+                       "max_abs_vs_plain": max(maxabs),
+                       "fallback_tiles": fb, "fallback_rate": fb / tiles,
+                       "l2": "outputs (106 MB planes) and activations (141 MB per layer) exceed L2",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "tensor", "kernel": "learned develop (7 conv launches + pack/output)",
+                         "achieved": flops / (ms_l / 1000.0) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                         "frac": flops / (ms_l / 1000.0) / 1e12 / peak, "traffic": None, "peak_source": pk,
+                         "algorithmic_flops_per_frame": flops},
+            "gpu_launches": int(launches),
+            "e2e": {"value": world * e2e_n / e2e_s, "unit": "frames/s",
+                    "h2d_bytes_per_step": int(np.mean([len(h[0]) for h in held])), "d2h_bytes_per_step": 12 * n,
+                    "note": "decode_frame from a host packet, learned develop, planes copied to pinned host memory"},
+        }
+        cl = clocks.summary()
+        if cl:
+            line["clocks"] = cl
+        if world == 1 and not args.no_cpu_baseline:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            import _oracle as O
+
+            threads = os.cpu_count() or 1
+            nf, t0 = 0, time.perf_counter()
+            while time.perf_counter() - t0 < 10.0 and nf < 16:
+                of = O.decode_frame(held[nf][0], 0, threads)
+                O.develop(of, O.params_new(of.header, of.quantizer), 2, True, threads)
+                nf += 1
+            el = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": nf / el, "unit": "frames/s", "cores": threads, "kind": "port",
+                                    "sample": f"{nf} held-out frames, oracle decode + plain develop (the reference "
+                                              f"has no learned develop), {threads} threads, {el:.1f} s"}
+        if args.save_model:
+            s.save(args.save_model)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+# 8K stream: 16 frames of 8192x4320 RGGB, version 1, qscale uniform in
+# [15, 45] (seed 4), noise sigma uniform in [4, 32]. One step = the 16
+# frames: one batch decode (the batch kernel's graph, replayed), then per
+# frame linearize and the learned develop to planar Rec.2020 into
+# preallocated device buffers, captured once as a CUDA graph and replayed.
+
+STREAM_W, STREAM_H, STREAM_N = 8192, 4320, 16
+
+
+def run_stream(args):
+    import torch
+
+    import proresraw_rs_b200 as P
+    from proresraw_rs_b200 import learned as L
+    from proresraw_rs_b200 import synth as S
+
+    world, rank, local = dist_setup(args.gpus)
+    if args.model and os.path.exists(args.model):
+        s = L.Surrogate.load(args.model)
+        train_s = 0.0
+    else:
+        s, _, train_s = train_for_bench(P, L, args.epochs)
+    rng = np.random.default_rng(4)
+    pkts = []
+    for k in range(STREAM_N):
+        sigma, q = float(rng.uniform(4, 32)), int(rng.integers(15, 46))
+        m = S.mosaic(STREAM_W, STREAM_H, S.RGGB, seed=4000 + k, sigma=sigma, white=4095)
+        spec = S.Spec(STREAM_W, STREAM_H, pattern=S.RGGB, version=1, white_level=4095, valid_tiles=True,
+                      wb=(1.9, 1.4), color_matrix=(0.61, 0.25, 0.10, 0.26, 0.89, -0.15, 0.02, -0.09, 1.17))
+        pkts.append(S.encode(spec, m, qscale=q, qscale_seed=k))
+    pkts = R.shard(pkts, rank, world) if world > 1 else pkts
+    nfr = len(pkts)
+    cw, ch = STREAM_W, STREAM_H
+    n = STREAM_W * STREAM_H
+    codes = [torch.empty(cw * ch, dtype=torch.uint16, device="cuda") for _ in range(nfr)]
+    lin = torch.empty(n, dtype=torch.uint16, device="cuda")
+    planes = [torch.empty(n, dtype=torch.float32, device="cuda") for _ in range(3)]
+    dec = P.BatchDecoder()
+    jobs = [P.BatchJob(p) for p in pkts]
+    res = dec.decode(jobs, codes)
+    assert not any(isinstance(r, P.Error) for r in res)
+    frames = res
+    prms = [P.DemosaicParams.new(f.header, f.quantizer()) for f in frames]
+    dp = s.device()
+    sur = L.Surrogate(s.params, s.noise_lo, s.noise_hi)
+    side = torch.cuda.Stream()
+
+    def develop_all(learned=True):
+        for f, prm in zip(frames, prms):
+            f.linearize_into(lin)
+            if learned:
+                L.develop_learned_planar_into(f, prm, P.Stage.REC2020, sur, planes, dev_params=dp,
+                                              count_fallback=False)
+            else:
+                P.develop_planar_into(f, prm, P.Stage.REC2020, planes)
+
+    # Warm up (allocations happen here), then capture the develop stage.
+    with torch.cuda.stream(side):
+        develop_all()
+        develop_all(False)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    k0 = P.kernel_launches()
+    with torch.cuda.graph(g, stream=side):
+        develop_all()
+    kernels_per_replay = P.kernel_launches() - k0  # launches recorded while capturing
+    gp = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(gp, stream=side):
+        develop_all(False)
+    torch.cuda.synchronize()
+
+    def step(graph):
+        dec.decode(jobs, codes)  # batch decode: upload, graph replay, statuses
+        graph.replay()
+
+    for k in range(max(3, args.warmup)):
+        step(g)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = P.kernel_launches()
+    dec_ms, dev_ms = 0.0, 0.0
+    with Clocks(torch.cuda.current_device()) as clocks:
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            dec.decode(jobs, codes)
+            dec_ms += dec.last_ms()
+            e0.record()
+            g.replay()
+            e1.record()
+            torch.cuda.synchronize()
+            dev_ms += e0.elapsed_time(e1)
+        wall = time.perf_counter() - t0
+    launches = P.kernel_launches() - launches0 + kernels_per_replay * args.steps
+    # Plain develop in the same pipeline, for comparison.
+    pd = 0.0
+    for k in range(max(2, args.steps // 2)):
+        e0.record()
+        gp.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        pd += e0.elapsed_time(e1)
+    pd /= max(2, args.steps // 2)
+    ms_step = R.reduce_max((dec_ms + dev_ms) / args.steps)
+    wall_step = R.reduce_max(wall / args.steps)
+    nall = int(R.reduce_sum(nfr))
+    if rank == 0:
+        peak, pk = peaks()
+        # Bytes per frame of the pipeline: packet + codes written, codes read
+        # twice (linearize, develop pack), linear values written, planes written.
+        pkt_bytes = float(np.mean([len(p) for p in pkts]))
+        alg = pkt_bytes + 2 * cw * ch + 2 * 2 * cw * ch + 2 * n + 12 * n
+        line = {
+            "metric": "8K stream frames/s (decode + linearize + learned develop to planar Rec.2020)",
+            "value": nall / (ms_step / 1000.0), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16 decode, bf16 network (f32 accumulate)", "data": "synthetic",
+            "config": {"workload": "16 x 8192x4320 RGGB v1, qscale U[15,45] seed 4, sigma U[4,32]; batch decode "
+                                   "graph + per-frame linearize + learned develop graph",
+                       "frames_per_step": nfr, "decode_ms_per_step": dec_ms / args.steps,
+                       "develop_ms_per_step": dev_ms / args.steps, "plain_develop_pipeline_ms_per_step": pd,
+                       "model_trained_seconds": train_s, "parallelism": f"replicas x{world}",
+                       "l2": "every frame's planes (425 MB) exceed L2"},
+            "roofline": {"bound": "hbm", "kernel": "whole pipeline", "achieved": alg * nfr / (ms_step / 1000.0) / 1e9,
+                         "peak": peak, "unit": "GB/s", "frac": alg * nfr / (ms_step / 1000.0) / 1e9 / peak,
+                         "traffic": None, "peak_source": f"{pk} hbm_gbs", "algorithmic_bytes_per_frame": alg},
+            "gpu_launches": int(launches),
+            "e2e": {"value": nall / wall_step, "unit": "frames/s", "h2d_bytes_per_step": int(sum(len(p) for p in pkts)),
+                    "d2h_bytes_per_step": 16 * nfr,
+                    "note": "batch decode from host packets (parse, upload, graph) + develop graph; planes stay on "
+                            "the device"},
+        }
+        cl = clocks.summary()
+        if cl:
+            line["clocks"] = cl
+        print(json.dumps(line), flush=True)
+    del g, gp
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="5k8", choices=["5k8", "mixed-batch"],
-                    help="5k8: the headline single-frame decode+develop; mixed-batch: 64 uneven frames per step")
+    ap.add_argument("--workload", default="5k8", choices=["5k8", "mixed-batch", "learned", "8k-stream"],
+                    help="5k8: the headline single-frame decode+develop; mixed-batch: 64 uneven frames per step; "
+                         "learned: surrogate develop of 4K frames (trains first); 8k-stream: 16 8K frames per step")
+    ap.add_argument("--epochs", type=int, default=8, help="training epochs for the learned workloads")
+    ap.add_argument("--save-model", default="", help="learned: save the trained surrogate (.npz)")
+    ap.add_argument("--model", default=os.path.join(ROOT, "proresraw_rs_b200", "data", "surrogate.npz"),
+                    help="8k-stream: a trained surrogate (.npz; default the packaged one); trained here if absent")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     args = ap.parse_args()
     if args.workload == "mixed-batch":
         return run_batch_reference(args) if args.impl == "reference" else run_batch(args)
+    if args.workload in ("learned", "8k-stream"):
+        if args.impl == "reference":
+            return run_reference(args)
+        return run_learned(args) if args.workload == "learned" else run_stream(args)
     if args.impl == "reference":
         return run_reference(args)
     return run(args)

@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import os
 from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
@@ -70,14 +71,25 @@ class Surrogate:
         return torch.from_numpy(np.ascontiguousarray(self.params, dtype=np.float32)).cuda()
 
 
+DEFAULT_MODEL = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "surrogate.npz")
+
+
+def default_surrogate() -> Surrogate:
+    """The packaged network: trained by this library on 4000 512x512 crops
+    of synthetic 4096x2160 frames (noise sigma 4..32, qscale 15..45)."""
+    return Surrogate.load(DEFAULT_MODEL)
+
+
 def _model(s: Surrogate, dev_params) -> _lib.CSgModel:
     return _lib.CSgModel(dev_params.data_ptr(), float(s.noise_lo), float(s.noise_hi))
 
 
 def develop_learned_planar_into(frame: Frame, params: DemosaicParams, stage: Stage, surrogate: Surrogate,
-                                out: Sequence, dev_params=None) -> int:
+                                out: Sequence, dev_params=None, count_fallback: bool = True) -> int:
     """develop_planar_into by the surrogate; returns the number of 32x32
-    tiles developed by the plain fallback."""
+    tiles developed by the plain fallback (count_fallback False: returns -1
+    and does not wait for the device, so the call can be captured in a CUDA
+    graph)."""
     torch = _torch()
     n = frame.header.width * frame.header.height
     if len(out) != 3 or any(int(o.numel()) != n for o in out):
@@ -88,9 +100,9 @@ def develop_learned_planar_into(frame: Frame, params: DemosaicParams, stage: Sta
     nfb = C.c_uint32()
     rc = _lib.lib().prr_develop_learned(ctx, C.byref(frame.header._c), C.byref(params._c()), int(stage),
                                         _dptr(frame.samples), C.byref(m), 1, _dptr(out[0]), _dptr(out[1]),
-                                        _dptr(out[2]), n, C.byref(nfb))
+                                        _dptr(out[2]), n, C.byref(nfb) if count_fallback else None)
     _check(rc, ctx=ctx)
-    return int(nfb.value)
+    return int(nfb.value) if count_fallback else -1
 
 
 def develop_learned(frame: Frame, stage: Stage, surrogate: Surrogate,
