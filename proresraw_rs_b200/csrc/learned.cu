@@ -81,7 +81,7 @@ constexpr size_t kPacked = packed_off(kLayers);
 
 constexpr int TX = 32, TY = 16;          // output tile of a conv CTA
 constexpr int WX = TX + 2, WY = TY + 2;  // input window
-constexpr int kConvThreads = 128;
+constexpr int kConvThreads = 256;  // two warpgroups; each reads back two of a tile's four M blocks
 constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
 
 template <int CIN, int COUT>
@@ -91,8 +91,7 @@ struct ConvCfg {
     static constexpr int RP = WX * 16;       // bytes per window row
     static constexpr int WIN_BYTES = C8 * CS;
     static constexpr int W_BYTES = 9 * C8 * COUT * 16;
-    static constexpr int SMEM = WIN_BYTES + W_BYTES;
-    static constexpr uint32_t TMEM_COLS = 4 * COUT;
+    static constexpr uint32_t TMEM_COLS = 4 * COUT;  // one tile's accumulators
     // Instruction descriptor, kind::f16: f32 accumulator (bits 4-5 = 1), A
     // and B bf16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17,
     // M >> 4 at bit 24.
@@ -219,129 +218,221 @@ __device__ __forceinline__ bool in_valid(const int4* valid, int b, int x, int y)
 }
 
 // --- the convolution on the tensor cores --------------------------------------
+//
+// Persistent: each CTA stages the layer's weights once and walks tiles
+// t = blockIdx.x, + gridDim.x, ... with two window buffers and two tensor-
+// memory accumulators. In iteration i it issues the MMAs of tile i + 1 (its
+// window already in shared memory) before the epilogue of tile i, and the
+// copies of window i + 2 right after, so copies, tensor-core work and the
+// epilogue of neighbouring tiles overlap.
 
-template <int CIN, int COUT, bool HEAD>
-__global__ void __launch_bounds__(kConvThreads) k_sg_conv(ConvArgs a) {
-    using C = ConvCfg<CIN, COUT>;
-    extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ uint32_t tmem_slot;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int img = blockIdx.z;
-    const int tx0 = blockIdx.x * TX, ty0 = blockIdx.y * TY;
-    uint8_t* win = smem;
-    uint8_t* wsm = smem + C::WIN_BYTES;
+struct TileCoord {
+    int img, tx0, ty0;
+};
 
-    // Window (zero outside the image) and weights: 16-byte asynchronous
-    // copies, all in flight at once (a source size of 0 fills zeros).
-    const uint4* xb = a.x + size_t(img) * C::C8 * a.H * a.W;
-    const uint32_t win_s = smem_u32(win), wsm_s = smem_u32(wsm);
-    for (int v = tid; v < C::C8 * WY * WX; v += kConvThreads) {
+__device__ __forceinline__ TileCoord tile_coord(int t, int tiles_x, int tiles_y) {
+    const int per = tiles_x * tiles_y;
+    TileCoord c;
+    c.img = t / per;
+    const int r = t - c.img * per;
+    c.ty0 = (r / tiles_x) * TY;
+    c.tx0 = (r % tiles_x) * TX;
+    return c;
+}
+
+// Window of a tile (zero outside the image): 16-byte asynchronous copies, a
+// source size of 0 filling zeros. One commit group per window.
+template <int C8>
+__device__ __forceinline__ void load_window(const ConvArgs& a, TileCoord tc, uint32_t dst) {
+    constexpr int CS = WY * WX * 16, RP = WX * 16;
+    const uint4* xb = a.x + size_t(tc.img) * C8 * a.H * a.W;
+    for (int v = threadIdx.x; v < C8 * WY * WX; v += kConvThreads) {
         const int c = v / (WY * WX), r = (v / WX) % WY, q = v % WX;
-        const int gy = ty0 - 1 + r, gx = tx0 - 1 + q;
+        const int gy = tc.ty0 - 1 + r, gx = tc.tx0 - 1 + q;
         const bool in = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
         const uint4* src = in ? xb + (size_t(c) * a.H + gy) * a.W + gx : xb;
-        cp_async16(win_s + uint32_t(c * C::CS + r * C::RP + q * 16), src, in);
+        cp_async16(dst + uint32_t(c * CS + r * RP + q * 16), src, in);
     }
-    for (int v = tid; v < C::W_BYTES / 16; v += kConvThreads) cp_async16(wsm_s + uint32_t(v * 16), a.w + v, true);
     asm volatile("cp.async.commit_group;" ::: "memory");
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    // The copies become visible to the tensor core's reads (async proxy).
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// One thread: the MMAs of a tile's four M blocks, then the commit. The
+// descriptors differ from the window's and the weights' base descriptors
+// only in the start address (bits 0-13, in 16-byte units, no carry: shared
+// addresses stay below 256 KB), so each is the base plus a constant.
+template <int CIN, int COUT>
+__device__ __forceinline__ void issue_tile(uint32_t win_a, uint32_t w_a, uint32_t tmem, uint32_t bar) {
+    using C = ConvCfg<CIN, COUT>;
+    const uint64_t a0 = sdesc(win_a, C::CS, C::RP), b0 = sdesc(w_a, COUT * 16, 128);
+#pragma unroll
+    for (int bk = 0; bk < 4; bk++) {
+#pragma unroll
+        for (int t = 0; t < 9; t++) {
+#pragma unroll
+            for (int h = 0; h < C::C8 / 2; h++) {
+                // A: rows m = 8 * r + i are window pixel (r + dy, 8 bk + i + dx),
+                // K chunk k = the window's chunk plane 2 h + k.
+                const uint32_t aoff = uint32_t((2 * h) * C::CS + (t / 3) * C::RP + (8 * bk + t % 3) * 16) >> 4;
+                // B: rows n = output channel, K chunk k = weights of input
+                // channels 16 h + 8 k .. + 7 at this tap.
+                const uint32_t boff = uint32_t((t * C::C8 + 2 * h) * COUT * 16) >> 4;
+                umma_f16(tmem + uint32_t(bk * COUT), a0 + aoff, b0 + boff, C::IDESC, (t | h) != 0 ? 1u : 0u);
+            }
+        }
+    }
+    umma_commit(bar);
+}
+
+template <int CIN, int COUT, bool HEAD>
+__device__ __forceinline__ void epilogue(const ConvArgs& a, TileCoord tc, uint32_t tmem, const float* bias) {
+    // A warp reads the 32 accumulator lanes of its quarter of the warpgroup
+    // (the lanes tensor memory lets it access), of its warpgroup's blocks.
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, quarter = warp & 3;
+    const int m = 32 * quarter + lane;  // accumulator row of this thread
+    const int py = tc.ty0 + (m >> 3);
+#pragma unroll 1
+    for (int bk = 2 * (warp >> 2); bk < 2 * (warp >> 2) + 2; bk++) {
+        const int px = tc.tx0 + 8 * bk + (m & 7);
+        uint32_t v[COUT];
+        tmem_load<COUT>(tmem + (uint32_t(32 * quarter) << 16) + uint32_t(bk * COUT), v);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (py >= a.H || px >= a.W) continue;
+        const bool keep = in_valid(a.valid, tc.img, px, py);
+        if (HEAD) {
+            float* o = a.yf + (size_t(tc.img) * kHead * a.H + py) * a.W + px;
+#pragma unroll
+            for (int c = 0; c < COUT; c++)
+                o[size_t(c) * a.H * a.W] = keep ? __fadd_rn(__uint_as_float(v[c]), bias[c]) : 0.0f;
+        } else {
+            uint4* o = a.y + (size_t(tc.img) * (COUT / 8) * a.H + py) * a.W + px;
+#pragma unroll
+            for (int c8 = 0; c8 < COUT / 8; c8++) {
+                float f[8];
+#pragma unroll
+                for (int e = 0; e < 8; e++) {
+                    const float s = __fadd_rn(__uint_as_float(v[c8 * 8 + e]), bias[c8 * 8 + e]);
+                    f[e] = keep ? fmaxf(s, 0.0f) : 0.0f;
+                }
+                o[size_t(c8) * a.H * a.W] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
+                                                       pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
+            }
+        }
+    }
+}
+
+template <int CIN, int COUT, bool HEAD>
+__global__ void __launch_bounds__(kConvThreads) k_sg_conv(ConvArgs a, int tiles_x, int tiles_y, int ntiles) {
+    using C = ConvCfg<CIN, COUT>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ float bias_s[COUT];
+    volatile __shared__ int aborted;  // a wait ran out: later waits and stores are skipped
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int first = blockIdx.x, stride = gridDim.x;
+    const int n = first < ntiles ? (ntiles - 1 - first) / stride + 1 : 0;  // this CTA's tiles
+    const uint32_t wsm = smem_u32(smem), win0 = wsm + C::W_BYTES, win1 = win0 + C::WIN_BYTES;
+    auto win_of = [&](int i) { return (i & 1) ? win1 : win0; };
+
+    // Weights once, then the first two windows.
+    for (int v = tid; v < C::W_BYTES / 16; v += kConvThreads) cp_async16(wsm + uint32_t(v * 16), a.w + v, true);
+    if (n > 0) load_window<C::C8>(a, tile_coord(first, tiles_x, tiles_y), win0);
+    else asm volatile("cp.async.commit_group;" ::: "memory");
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                     "r"(C::TMEM_COLS));
+                     "r"(2 * C::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        aborted = 0;
     }
+    if (tid < COUT) bias_s[tid] = a.bias[tid];
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    const uint32_t bar = smem_u32(&mbar);
+    const uint32_t bar[2] = {smem_u32(&mbar[0]), smem_u32(&mbar[1])};
+    auto acc_of = [&](int i) { return tmem + uint32_t((i & 1) * C::TMEM_COLS); };
+    if (n > 0 && tid == 0) issue_tile<CIN, COUT>(win0, wsm, acc_of(0), bar[0]);
+    if (n > 1) load_window<C::C8>(a, tile_coord(first + stride, tiles_x, tiles_y), win1);
 
-    if (tid == 0) {
-        const uint32_t win_a = smem_u32(win), w_a = smem_u32(wsm);
+    int issued = n > 0 ? 1 : 0;  // tiles whose MMAs are issued
 #pragma unroll 1
-        for (int bk = 0; bk < 4; bk++) {
-#pragma unroll 1
-            for (int t = 0; t < 9; t++) {
-                const int dy = t / 3, dx = t % 3;
-#pragma unroll
-                for (int h = 0; h < C::C8 / 2; h++) {
-                    // A: rows m = 8 * r + i are window pixel (r + dy, 8 bk + i + dx),
-                    // K chunk k = the window's chunk plane 2 h + k.
-                    const uint32_t aa = win_a + uint32_t((2 * h) * C::CS + dy * C::RP + (8 * bk + dx) * 16);
-                    // B: rows n = output channel, K chunk k = weights of input
-                    // channels 16 h + 8 k .. + 7 at this tap.
-                    const uint32_t ba = w_a + uint32_t((t * C::C8 + 2 * h) * COUT * 16);
-                    umma_f16(tmem + uint32_t(bk * COUT), sdesc(aa, C::CS, C::RP), sdesc(ba, COUT * 16, 128),
-                             C::IDESC, (t | h) != 0 ? 1u : 0u);
-                }
-            }
+    for (int i = 0; i < n; i++) {
+        if (i + 1 < n) {
+            // Window i + 1 has landed (this thread's copies, then everyone's);
+            // the epilogue of tile i - 1 has read accumulator (i + 1) & 1.
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tc_fence_before();
+            __syncthreads();
+            tc_fence_after();
+            if (tid == 0 && !aborted) issue_tile<CIN, COUT>(win_of(i + 1), wsm, acc_of(i + 1), bar[(i + 1) & 1]);
+            issued = i + 2;
         }
-        umma_commit(bar);
-    }
-    // The epilogue's tensor-memory loads are warp-collective: every thread
-    // takes the same branch.
-    const bool ok = __syncthreads_and(mbar_wait(bar, 0, kWaitNs) ? 1 : 0) != 0;
-    if (!ok) {
-        if (tid == 0) atomicOr(a.error, 1u);
-        mbar_wait(bar, 0, kWaitNs);  // let the issued work finish before the memory is freed
-    }
-    tc_fence_after();
-    if (ok) {
-        const int m = 32 * warp + lane;  // accumulator row of this thread
-        const int py = ty0 + (m >> 3);
-#pragma unroll 1
-        for (int bk = 0; bk < 4; bk++) {
-            const int px = tx0 + 8 * bk + (m & 7);
-            uint32_t v[COUT];
-            tmem_load<COUT>(tmem + (uint32_t(32 * warp) << 16) + uint32_t(bk * COUT), v);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (py >= a.H || px >= a.W) continue;
-            const bool keep = in_valid(a.valid, img, px, py);
-            if (HEAD) {
-                float* o = a.yf + (size_t(img) * kHead * a.H + py) * a.W + px;
-#pragma unroll
-                for (int c = 0; c < COUT; c++)
-                    o[size_t(c) * a.H * a.W] = keep ? __fadd_rn(__uint_as_float(v[c]), __ldg(a.bias + c)) : 0.0f;
-            } else {
-                uint4* o = a.y + (size_t(img) * (COUT / 8) * a.H + py) * a.W + px;
-#pragma unroll
-                for (int c8 = 0; c8 < COUT / 8; c8++) {
-                    float f[8];
-#pragma unroll
-                    for (int e = 0; e < 8; e++) {
-                        const float s = __fadd_rn(__uint_as_float(v[c8 * 8 + e]), __ldg(a.bias + c8 * 8 + e));
-                        f[e] = keep ? fmaxf(s, 0.0f) : 0.0f;
-                    }
-                    o[size_t(c8) * a.H * a.W] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
-                                                           pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
-                }
-            }
+        // Epilogue of tile i, while thread 0 may still be issuing tile i + 1:
+        // the accumulator is complete when its barrier's (i / 2)-th phase is.
+        // The warp-collective loads need the same branch in a whole warp.
+        bool ok = !aborted && mbar_wait(bar[i & 1], uint32_t((i >> 1) & 1), kWaitNs);
+        ok = __all_sync(0xFFFFFFFFu, ok);
+        if (!ok && !aborted) {
+            aborted = 1;
+            atomicOr(a.error, 1u);
         }
+        if (ok) {
+            tc_fence_after();
+            epilogue<CIN, COUT, HEAD>(a, tile_coord(first + i * stride, tiles_x, tiles_y), acc_of(i), bias_s);
+            tc_fence_before();
+        }
+        // Window i + 2 reuses the buffer of window i, which tile i's MMAs
+        // (complete above) no longer read.
+        if (i + 2 < n && ok)
+            load_window<C::C8>(a, tile_coord(first + (i + 2) * stride, tiles_x, tiles_y), win_of(i));
+        else
+            asm volatile("cp.async.commit_group;" ::: "memory");
     }
+    __syncthreads();
+    if (aborted && issued > 0) {
+        // Let the issued MMAs finish (bounded) before the memory is freed:
+        // they complete in order, so the last commit covers them all.
+        const int j = issued - 1;
+        mbar_wait(bar[j & 1], uint32_t((j >> 1) & 1), kWaitNs);
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     tc_fence_before();
     __syncthreads();
-    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::TMEM_COLS));
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * C::TMEM_COLS));
 }
 
 template <int CIN, int COUT, bool HEAD>
 cudaError_t conv_launch(const ConvArgs& a, int images, cudaStream_t s) {
     using C = ConvCfg<CIN, COUT>;
-    static bool attr = false;  // per process; the attribute is per device and set on first use
-    if (!attr) {
-        const cudaError_t e = cudaFuncSetAttribute(k_sg_conv<CIN, COUT, HEAD>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+    // At least 80 KB of shared memory per CTA, so that no more than two CTAs
+    // share an SM: two CTAs' 2 x 128 accumulator columns fill its 512, and a
+    // third CTA's allocation would wait for one of them to finish.
+    constexpr int smem = std::max(C::W_BYTES + 2 * C::WIN_BYTES, 80 * 1024);
+    static int sms = 0;  // per process: the attribute and SM count of the first device used
+    if (sms == 0) {
+        cudaError_t e = cudaFuncSetAttribute(k_sg_conv<CIN, COUT, HEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             smem);
         if (e != cudaSuccess) return e;
-        attr = true;
+        int dev = 0;
+        e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
     }
-    dim3 grid((a.W + TX - 1) / TX, (a.H + TY - 1) / TY, images);
-    k_sg_conv<CIN, COUT, HEAD><<<grid, kConvThreads, C::SMEM, s>>>(a);
+    const int tiles_x = (a.W + TX - 1) / TX, tiles_y = (a.H + TY - 1) / TY;
+    const int ntiles = tiles_x * tiles_y * images;
+    // Two CTAs per SM: 2 x (weights + two windows) of shared memory and
+    // 2 x 2 accumulators of tensor memory fit.
+    const int grid = std::max(1, std::min(ntiles, 2 * sms));
+    k_sg_conv<CIN, COUT, HEAD><<<grid, kConvThreads, smem, s>>>(a, tiles_x, tiles_y, ntiles);
     count_launch();
     return cudaGetLastError();
 }
