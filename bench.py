@@ -422,11 +422,11 @@ def measure_e2e(args, L, _lib, pkts, n, world):
 BATCH_N, BATCH_SEED = 64, 2
 
 
-def batch_jobs():
+def batch_jobs(n=BATCH_N):
     import proresraw_rs_b200 as P
     from proresraw_rs_b200 import synth as S
 
-    items = S.mixed_batch(BATCH_N, seed=BATCH_SEED)
+    items = S.mixed_batch(n, seed=BATCH_SEED)
     jobs = [P.BatchJob(it.packet, None if it.scale == 0 else P.Scale(it.scale), P.Idct.APPLE,
                        P.Greens(it.greens)) for it in items]
     return items, jobs
@@ -475,7 +475,8 @@ def run_batch(args):
 
     world, rank, local = dist_setup(args.gpus)
     L = _lib.lib()
-    items, jobs = batch_jobs()
+    items, jobs = batch_jobs(args.batch_frames)
+    nb = len(items)
     outs = []
     for it in items:
         cw, ch = (it.width + 15) // 16 * 16, (it.height + 15) // 16 * 16
@@ -484,7 +485,10 @@ def run_batch(args):
     dec = P.BatchDecoder()
     res = dec.decode(jobs, outs)
     assert not any(isinstance(r, P.Error) for r in res)
-    cfg, tuned_ms = dec.tune(jobs, reps=2)
+    if args.no_tune:
+        cfg, tuned_ms = dec.get_config(dec.bucket(jobs)), None
+    else:
+        cfg, tuned_ms = dec.tune(jobs, reps=2)
     for _ in range(max(3, args.warmup)):
         dec.decode(jobs, outs)
     if world > 1:
@@ -503,7 +507,7 @@ def run_batch(args):
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
     ms_max, wall_max = float(t[0].item()), float(t[1].item())
-    value = world * args.steps * BATCH_N / (ms_max / 1000.0)
+    value = world * args.steps * nb / (ms_max / 1000.0)
     if rank == 0:
         peak, peak_kind = peaks()
         alg = batch_bytes(items)
@@ -512,7 +516,7 @@ def run_batch(args):
             "metric": BATCH_METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-            "config": {"workload": BATCH_WORKLOAD, "frames_per_step": BATCH_N,
+            "config": {"workload": BATCH_WORKLOAD.replace("64 frames", f"{nb} frames"), "frames_per_step": nb,
                        "packet_bytes_per_step": sum(len(it.packet) for it in items),
                        "l2": "inputs+outputs > L2 (about 1 GB written per step)",
                        "parallelism": f"replicas x{world}",
@@ -521,9 +525,9 @@ def run_batch(args):
                          "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                          "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg},
             "gpu_launches": int(launches),
-            "e2e": {"value": world * args.steps * BATCH_N / wall_max, "unit": "frames/s",
+            "e2e": {"value": world * args.steps * nb / wall_max, "unit": "frames/s",
                     "h2d_bytes_per_step": sum(len(it.packet) for it in items),
-                    "d2h_bytes_per_step": 16 * BATCH_N,
+                    "d2h_bytes_per_step": 16 * nb,
                     "note": "BatchDecoder.decode from host packets: parse, upload, kernels, statuses back; "
                             "frames stay on the device"},
         }
@@ -544,7 +548,7 @@ def run_batch(args):
 def run_batch_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    items, _ = batch_jobs()
+    items, _ = batch_jobs(args.batch_frames)
     budget = max(10.0, 2.0 * args.steps)
     v, n, el, threads = batch_cpu(items, budget)
     line = {
@@ -885,6 +889,8 @@ def main():
     ap.add_argument("--save-model", default="", help="learned: save the trained surrogate (.npz)")
     ap.add_argument("--model", default=os.path.join(ROOT, "proresraw_rs_b200", "data", "surrogate.npz"),
                     help="8k-stream: a trained surrogate (.npz; default the packaged one); trained here if absent")
+    ap.add_argument("--batch-frames", type=int, default=BATCH_N, help="mixed-batch: frames per batch")
+    ap.add_argument("--no-tune", action="store_true", help="mixed-batch: skip the autotuner (default shape)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     args = ap.parse_args()

@@ -236,3 +236,49 @@ def psnr(a: np.ndarray, b: np.ndarray, peak: float = 1.0) -> float:
 
 def max_abs(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.max(np.abs(np.asarray(a, dtype=np.float64) - np.asarray(b, dtype=np.float64))))
+
+
+def _main(argv=None) -> int:
+    """Develop a synthetic frame with the packaged network and time it:
+    python -m proresraw_rs_b200.learned [--width W] [--height H] [--reps N]"""
+    import argparse
+    import time
+
+    from . import synth as S
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--width", type=int, default=4096)
+    ap.add_argument("--height", type=int, default=2160)
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--seed", type=int, default=7)
+    a = ap.parse_args(argv)
+    torch = _torch()
+    from . import decode_frame, develop_planar_into
+
+    m = S.mosaic(a.width, a.height, S.RGGB, seed=a.seed, sigma=16.0, white=4095)
+    spec = S.Spec(a.width, a.height, pattern=S.RGGB, alignment=2, white_level=4095, valid_tiles=True, wb=(1.9, 1.4),
+                  color_matrix=(0.61, 0.25, 0.10, 0.26, 0.89, -0.15, 0.02, -0.09, 1.17))
+    f = decode_frame(S.encode(spec, m, qscale=30, qscale_seed=a.seed))
+    s = default_surrogate()
+    n = a.width * a.height
+    out = [torch.empty(n, dtype=torch.float32, device="cuda") for _ in range(3)]
+    prm = DemosaicParams.new(f.header, f.quantizer())
+    dp = s.device()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    develop_learned_planar_into(f, prm, Stage.REC2020, s, out, dev_params=dp)
+    torch.cuda.synchronize()
+    ev[0].record()
+    for _ in range(a.reps):
+        develop_learned_planar_into(f, prm, Stage.REC2020, s, out, dev_params=dp, count_fallback=False)
+    ev[1].record()
+    for _ in range(a.reps):
+        develop_planar_into(f, prm, Stage.REC2020, out)
+    ev[2].record()
+    torch.cuda.synchronize()
+    print(f"{a.width}x{a.height}: learned develop {ev[0].elapsed_time(ev[1]) / a.reps:.3f} ms, "
+          f"plain develop {ev[1].elapsed_time(ev[2]) / a.reps:.3f} ms")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(_main())
