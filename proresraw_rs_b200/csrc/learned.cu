@@ -47,6 +47,7 @@
 // per CTA and added with atomics. Adam keeps f32 master weights; the tensor
 // core copy is re-packed to bf16 before each forward.
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -219,12 +220,24 @@ __device__ __forceinline__ bool in_valid(const int4* valid, int b, int x, int y)
 
 // --- the convolution on the tensor cores --------------------------------------
 //
-// Persistent: each CTA stages the layer's weights once and walks tiles
-// t = blockIdx.x, + gridDim.x, ... with two window buffers and two tensor-
-// memory accumulators. In iteration i it issues the MMAs of tile i + 1 (its
-// window already in shared memory) before the epilogue of tile i, and the
-// copies of window i + 2 right after, so copies, tensor-core work and the
-// epilogue of neighbouring tiles overlap.
+// Warp-specialized and persistent. Each CTA walks tiles t = blockIdx.x,
+// + gridDim.x, ... with:
+//  - a producer warp: the layer's weights once (bulk copy), then each tile's
+//    input window by one TMA tensor load (box 8 x 34 x 18 x CIN/8 of the
+//    activation tensor, zero-filled outside the image) into a two-stage ring;
+//  - an MMA warp: per tile, 4 blocks x 9 taps x CIN/16 tcgen05.mma into one
+//    of two tensor-memory accumulators, then commits that free the window
+//    stage and publish the accumulator;
+//  - eight epilogue warps: tcgen05.ld of the accumulator (a warp reads the 32
+//    lanes of its quarter, for two of the four blocks), bias, ReLU, bf16
+//    stores; then they hand the accumulator back.
+// Stages and accumulators are passed by mbarriers (full/empty rings). Every
+// wait is bounded; a wait that runs out sets the error flag and makes every
+// role stop at its next step.
+
+constexpr int kEpiWarps = 8, kProducerWarp = 8, kMmaWarp = 9;
+constexpr int kWsThreads = 32 * (kEpiWarps + 2);
+constexpr int kStages = 2, kAccs = 2;
 
 struct TileCoord {
     int img, tx0, ty0;
@@ -240,28 +253,39 @@ __device__ __forceinline__ TileCoord tile_coord(int t, int tiles_x, int tiles_y)
     return c;
 }
 
-// Window of a tile (zero outside the image): 16-byte asynchronous copies, a
-// source size of 0 filling zeros. One commit group per window.
-template <int C8>
-__device__ __forceinline__ void load_window(const ConvArgs& a, TileCoord tc, uint32_t dst) {
-    constexpr int CS = WY * WX * 16, RP = WX * 16;
-    const uint4* xb = a.x + size_t(tc.img) * C8 * a.H * a.W;
-    for (int v = threadIdx.x; v < C8 * WY * WX; v += kConvThreads) {
-        const int c = v / (WY * WX), r = (v / WX) % WY, q = v % WX;
-        const int gy = tc.ty0 - 1 + r, gx = tc.tx0 - 1 + q;
-        const bool in = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W;
-        const uint4* src = in ? xb + (size_t(c) * a.H + gy) * a.W + gx : xb;
-        cp_async16(dst + uint32_t(c * CS + r * RP + q * 16), src, in);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(bar) : "memory");
 }
 
-// One thread: the MMAs of a tile's four M blocks, then the commit. The
-// descriptors differ from the window's and the weights' base descriptors
-// only in the start address (bits 0-13, in 16-byte units, no carry: shared
-// addresses stay below 256 KB), so each is the base plus a constant.
+// One TMA tensor load of a window: coordinates (element, x, y, plane).
+__device__ __forceinline__ void tma_window(const CUtensorMap* map, uint32_t dst, uint32_t bar, int x, int y,
+                                           int plane) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+        "[%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(0), "r"(x), "r"(y), "r"(plane)
+        : "memory");
+}
+
+// Contiguous global -> shared bulk copy (16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// One thread: the MMAs of a tile's four M blocks. The descriptors differ
+// from the window's and the weights' base descriptors only in the start
+// address (bits 0-13, 16-byte units, no carry: shared addresses stay below
+// 256 KB), so each is the base plus a constant.
 template <int CIN, int COUT>
-__device__ __forceinline__ void issue_tile(uint32_t win_a, uint32_t w_a, uint32_t tmem, uint32_t bar) {
+__device__ __forceinline__ void issue_tile(uint32_t win_a, uint32_t w_a, uint32_t tmem) {
     using C = ConvCfg<CIN, COUT>;
     const uint64_t a0 = sdesc(win_a, C::CS, C::RP), b0 = sdesc(w_a, COUT * 16, 128);
 #pragma unroll
@@ -280,13 +304,12 @@ __device__ __forceinline__ void issue_tile(uint32_t win_a, uint32_t w_a, uint32_
             }
         }
     }
-    umma_commit(bar);
 }
 
 template <int CIN, int COUT, bool HEAD>
 __device__ __forceinline__ void epilogue(const ConvArgs& a, TileCoord tc, uint32_t tmem, const float* bias) {
-    // A warp reads the 32 accumulator lanes of its quarter of the warpgroup
-    // (the lanes tensor memory lets it access), of its warpgroup's blocks.
+    // A warp reads the 32 accumulator lanes of its quarter (the lanes tensor
+    // memory lets it access), for two of the four blocks.
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, quarter = warp & 3;
     const int m = 32 * quarter + lane;  // accumulator row of this thread
     const int py = tc.ty0 + (m >> 3);
@@ -321,102 +344,160 @@ __device__ __forceinline__ void epilogue(const ConvArgs& a, TileCoord tc, uint32
 }
 
 template <int CIN, int COUT, bool HEAD>
-__global__ void __launch_bounds__(kConvThreads) k_sg_conv(ConvArgs a, int tiles_x, int tiles_y, int ntiles) {
+__global__ void __launch_bounds__(kWsThreads) k_sg_conv(const __grid_constant__ CUtensorMap tmap, ConvArgs a,
+                                                         int tiles_x, int tiles_y, int ntiles) {
     using C = ConvCfg<CIN, COUT>;
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ __align__(8) uint64_t bars[2 * kStages + 2 * kAccs + 1];
     __shared__ uint32_t tmem_slot;
     __shared__ float bias_s[COUT];
-    volatile __shared__ int aborted;  // a wait ran out: later waits and stores are skipped
-    const int tid = threadIdx.x, warp = tid >> 5;
+    volatile __shared__ int aborted;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int first = blockIdx.x, stride = gridDim.x;
     const int n = first < ntiles ? (ntiles - 1 - first) / stride + 1 : 0;  // this CTA's tiles
-    const uint32_t wsm = smem_u32(smem), win0 = wsm + C::W_BYTES, win1 = win0 + C::WIN_BYTES;
-    auto win_of = [&](int i) { return (i & 1) ? win1 : win0; };
-
-    // Weights once, then the first two windows.
-    for (int v = tid; v < C::W_BYTES / 16; v += kConvThreads) cp_async16(wsm + uint32_t(v * 16), a.w + v, true);
-    if (n > 0) load_window<C::C8>(a, tile_coord(first, tiles_x, tiles_y), win0);
-    else asm volatile("cp.async.commit_group;" ::: "memory");
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                     "r"(2 * C::TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
+    // Weights, then the window stages, 128-byte aligned.
+    const uint32_t wsm = smem_u32(smem);
+    const uint32_t win0 = wsm + uint32_t((C::W_BYTES + 127) & ~127);
+    const uint32_t win_stride = uint32_t((C::WIN_BYTES + 127) & ~127);
+    auto bar = [&](int i) { return smem_u32(&bars[i]); };
+    // bars: full[s] = 0..1, empty[s] = 2..3, tfull[a] = 4..5, tempty[a] = 6..7, weights = 8.
+    const uint32_t full0 = bar(0), empty0 = bar(kStages), tfull0 = bar(2 * kStages), tempty0 = bar(2 * kStages + kAccs),
+                   wbar = bar(2 * kStages + 2 * kAccs);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(full0 + 8 * s, 1);   // the producer's expect_tx arrival
+            mbar_init(empty0 + 8 * s, 1);  // the MMA warp's commit
+        }
+        for (int q = 0; q < kAccs; q++) {
+            mbar_init(tfull0 + 8 * q, 1);           // the MMA warp's commit
+            mbar_init(tempty0 + 8 * q, kEpiWarps);  // one arrival per epilogue warp
+        }
+        mbar_init(wbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         aborted = 0;
     }
     if (tid < COUT) bias_s[tid] = a.bias[tid];
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(kAccs * C::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    const uint32_t bar[2] = {smem_u32(&mbar[0]), smem_u32(&mbar[1])};
-    auto acc_of = [&](int i) { return tmem + uint32_t((i & 1) * C::TMEM_COLS); };
-    if (n > 0 && tid == 0) issue_tile<CIN, COUT>(win0, wsm, acc_of(0), bar[0]);
-    if (n > 1) load_window<C::C8>(a, tile_coord(first + stride, tiles_x, tiles_y), win1);
+    int issued = 0;  // MMA warp: tiles whose MMAs are issued
 
-    int issued = n > 0 ? 1 : 0;  // tiles whose MMAs are issued
-#pragma unroll 1
-    for (int i = 0; i < n; i++) {
-        if (i + 1 < n) {
-            // Window i + 1 has landed (this thread's copies, then everyone's);
-            // the epilogue of tile i - 1 has read accumulator (i + 1) & 1.
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            tc_fence_before();
-            __syncthreads();
+    if (warp == kProducerWarp) {
+        if (lane == 0) {
+            mbar_expect_tx(wbar, uint32_t(C::W_BYTES));
+            bulk_copy(wsm, a.w, uint32_t(C::W_BYTES), wbar);
+            for (int i = 0; i < n; i++) {
+                const int s = i % kStages;
+                // The stage is free once the MMAs of tile i - kStages are done
+                // (the first round passes: its parity refers to the phase
+                // before the barrier's first).
+                if (aborted || !mbar_wait(empty0 + 8 * s, uint32_t(((i / kStages) & 1) ^ 1), kWaitNs)) {
+                    if (!aborted) atomicOr(a.error, 1u);
+                    aborted = 1;
+                    break;
+                }
+                const TileCoord tc = tile_coord(first + i * stride, tiles_x, tiles_y);
+                mbar_expect_tx(full0 + 8 * s, uint32_t(C::WIN_BYTES));
+                tma_window(&tmap, win0 + uint32_t(s) * win_stride, full0 + 8 * s, tc.tx0 - 1, tc.ty0 - 1,
+                           tc.img * C::C8);
+            }
+        }
+    } else if (warp == kMmaWarp) {
+        if (lane == 0) {
+            bool ok = mbar_wait(wbar, 0, kWaitNs);
+            for (int i = 0; ok && i < n; i++) {
+                const int s = i % kStages, q = i % kAccs;
+                ok = !aborted && mbar_wait(full0 + 8 * s, uint32_t((i / kStages) & 1), kWaitNs) &&
+                     mbar_wait(tempty0 + 8 * q, uint32_t(((i / kAccs) & 1) ^ 1), kWaitNs);
+                if (!ok) break;
+                tc_fence_after();
+                issue_tile<CIN, COUT>(win0 + uint32_t(s) * win_stride, wsm, tmem + uint32_t(q) * C::TMEM_COLS);
+                umma_commit(empty0 + 8 * s);  // the window stage, once these MMAs have read it
+                umma_commit(tfull0 + 8 * q);  // the accumulator, once they are done
+                issued = i + 1;
+            }
+            if (!ok) {
+                if (!aborted) atomicOr(a.error, 1u);
+                aborted = 1;
+            }
+        }
+    } else {
+        for (int i = 0; i < n; i++) {
+            const int q = i % kAccs;
+            bool ok = !aborted && mbar_wait(tfull0 + 8 * q, uint32_t((i / kAccs) & 1), kWaitNs);
+            ok = __all_sync(0xFFFFFFFFu, ok);  // the warp-collective loads need one branch per warp
+            if (!ok) {
+                if (lane == 0) {
+                    if (!aborted) atomicOr(a.error, 1u);
+                    aborted = 1;
+                }
+                break;
+            }
             tc_fence_after();
-            if (tid == 0 && !aborted) issue_tile<CIN, COUT>(win_of(i + 1), wsm, acc_of(i + 1), bar[(i + 1) & 1]);
-            issued = i + 2;
-        }
-        // Epilogue of tile i, while thread 0 may still be issuing tile i + 1:
-        // the accumulator is complete when its barrier's (i / 2)-th phase is.
-        // The warp-collective loads need the same branch in a whole warp.
-        bool ok = !aborted && mbar_wait(bar[i & 1], uint32_t((i >> 1) & 1), kWaitNs);
-        ok = __all_sync(0xFFFFFFFFu, ok);
-        if (!ok && !aborted) {
-            aborted = 1;
-            atomicOr(a.error, 1u);
-        }
-        if (ok) {
-            tc_fence_after();
-            epilogue<CIN, COUT, HEAD>(a, tile_coord(first + i * stride, tiles_x, tiles_y), acc_of(i), bias_s);
+            epilogue<CIN, COUT, HEAD>(a, tile_coord(first + i * stride, tiles_x, tiles_y),
+                                      tmem + uint32_t(q) * C::TMEM_COLS, bias_s);
             tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty0 + 8 * q);
         }
-        // Window i + 2 reuses the buffer of window i, which tile i's MMAs
-        // (complete above) no longer read.
-        if (i + 2 < n && ok)
-            load_window<C::C8>(a, tile_coord(first + (i + 2) * stride, tiles_x, tiles_y), win_of(i));
-        else
-            asm volatile("cp.async.commit_group;" ::: "memory");
     }
     __syncthreads();
-    if (aborted && issued > 0) {
+    if (aborted && tid == kMmaWarp * 32 && issued > 0) {
         // Let the issued MMAs finish (bounded) before the memory is freed:
         // they complete in order, so the last commit covers them all.
         const int j = issued - 1;
-        mbar_wait(bar[j & 1], uint32_t((j >> 1) & 1), kWaitNs);
+        mbar_wait(tfull0 + 8 * (j % kAccs), uint32_t((j / kAccs) & 1), kWaitNs);
     }
-    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    if (aborted && tid == kProducerWarp * 32) {
+        // Let the issued window loads land (bounded) before the CTA exits.
+        for (int s = 0; s < kStages; s++) mbar_wait(full0 + 8 * s, 0, kWaitNs / 8);
+    }
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * C::TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kAccs * C::TMEM_COLS));
+}
+
+// cuTensorMapEncodeTiled, looked up once through the runtime (no link
+// against the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+cudaError_t encode_window_map(CUtensorMap* map, const void* x, int c8, int H, int W, int images) {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return e != cudaSuccess ? e : cudaErrorUnknown;
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    // The activation tensor as 4-D bf16: 8 channels of a chunk, x, y, and
+    // (image, chunk) planes; the window box covers one image's chunks.
+    const cuuint64_t dims[4] = {8, cuuint64_t(W), cuuint64_t(H), cuuint64_t(c8) * cuuint64_t(images)};
+    const cuuint64_t strides[3] = {16, cuuint64_t(W) * 16, cuuint64_t(W) * cuuint64_t(H) * 16};
+    const cuuint32_t box[4] = {8, WX, WY, cuuint32_t(c8)};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 template <int CIN, int COUT, bool HEAD>
 cudaError_t conv_launch(const ConvArgs& a, int images, cudaStream_t s) {
     using C = ConvCfg<CIN, COUT>;
-    // At least 80 KB of shared memory per CTA, so that no more than two CTAs
-    // share an SM: two CTAs' 2 x 128 accumulator columns fill its 512, and a
-    // third CTA's allocation would wait for one of them to finish.
-    constexpr int smem = std::max(C::W_BYTES + 2 * C::WIN_BYTES, 80 * 1024);
+    // Weights and two window stages; at least 80 KB, so that no more than
+    // two CTAs share an SM: two CTAs' 2 x 4 x COUT accumulator columns fit
+    // in its 512, and a third CTA's allocation would wait for one of them.
+    constexpr int smem = std::max(((C::W_BYTES + 127) & ~127) + kStages * ((C::WIN_BYTES + 127) & ~127), 80 * 1024);
     static int sms = 0;  // per process: the attribute and SM count of the first device used
     if (sms == 0) {
         cudaError_t e = cudaFuncSetAttribute(k_sg_conv<CIN, COUT, HEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -427,12 +508,13 @@ cudaError_t conv_launch(const ConvArgs& a, int images, cudaStream_t s) {
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
     }
+    alignas(64) CUtensorMap map;
+    const cudaError_t em = encode_window_map(&map, a.x, C::C8, a.H, a.W, images);
+    if (em != cudaSuccess) return em;
     const int tiles_x = (a.W + TX - 1) / TX, tiles_y = (a.H + TY - 1) / TY;
     const int ntiles = tiles_x * tiles_y * images;
-    // Two CTAs per SM: 2 x (weights + two windows) of shared memory and
-    // 2 x 2 accumulators of tensor memory fit.
     const int grid = std::max(1, std::min(ntiles, 2 * sms));
-    k_sg_conv<CIN, COUT, HEAD><<<grid, kConvThreads, smem, s>>>(a, tiles_x, tiles_y, ntiles);
+    k_sg_conv<CIN, COUT, HEAD><<<grid, kWsThreads, smem, s>>>(map, a, tiles_x, tiles_y, ntiles);
     count_launch();
     return cudaGetLastError();
 }
