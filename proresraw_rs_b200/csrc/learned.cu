@@ -101,6 +101,25 @@ struct ConvCfg {
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "tcgen05 shape");
 };
 
+// The develop output written by the head's epilogue (inference): picture
+// pixels from network-frame quads.
+struct RgbOut {
+    const float* base;  // [3][hq][wq], network frame: each quad's colour
+    int w, h;           // picture
+    int rr, rc;         // mirrors of the network frame
+    int has_matrix;
+    float m[9];
+    int layout;
+    float* r;
+    float* g;
+    float* b;
+    const uint8_t* fallback;  // per 32x32 picture tile: developed by the plain kernel instead
+    int tiles_x;
+};
+
+// Epilogue modes of the convolution.
+enum : int { kHidden = 0, kHeadF32 = 1, kHeadRgb = 2 };
+
 struct ConvArgs {
     const uint4* x;     // bf16 chunks [image][CIN/8][H][W]
     const uint4* w;     // the layer's packed weights [tap][CIN/8][COUT] x 8 bf16
@@ -306,8 +325,47 @@ __device__ __forceinline__ void issue_tile(uint32_t win_a, uint32_t w_a, uint32_
     }
 }
 
-template <int CIN, int COUT, bool HEAD>
-__device__ __forceinline__ void epilogue(const ConvArgs& a, TileCoord tc, uint32_t tmem, const float* bias) {
+// Head channel c * 4 + 2 sy + sx of network quad (i, j), plus the quad's
+// colour, is network pixel (2 i + sx, 2 j + sy), mirrored back to the
+// picture; min(., 1), the matrix (src/demosaic.rs:700-720 for its operation
+// order), and the store.
+__device__ __forceinline__ void rgb_quad(const RgbOut& o, int i, int j, int wq, int hq, const float* hv) {
+    const size_t plane = size_t(wq) * hq, q = size_t(j) * wq + i;
+    const float b0 = o.base[q], b1 = o.base[plane + q], b2 = o.base[2 * plane + q];
+    const int X0 = o.rc ? o.w - 1 - 2 * i : 2 * i, Y0 = o.rr ? o.h - 1 - 2 * j : 2 * j;
+    if (o.fallback && o.fallback[(Y0 / kDevelopTile) * o.tiles_x + X0 / kDevelopTile]) return;
+#pragma unroll
+    for (int sy = 0; sy < 2; sy++)
+#pragma unroll
+        for (int sx = 0; sx < 2; sx++) {
+            const int X = o.rc ? X0 - sx : X0 + sx, Y = o.rr ? Y0 - sy : Y0 + sy;
+            if (X < 0 || Y < 0 || X >= o.w || Y >= o.h) continue;
+            const int sidx = sy * 2 + sx;
+            float r = fminf(__fadd_rn(hv[0 + sidx], b0), 1.0f);
+            float g = fminf(__fadd_rn(hv[4 + sidx], b1), 1.0f);
+            float b = fminf(__fadd_rn(hv[8 + sidx], b2), 1.0f);
+            if (o.has_matrix) {
+                const float r0 = r, g0 = g, bb0 = b;
+                r = __fmaf_rn(bb0, o.m[2], __fmaf_rn(r0, o.m[0], __fmul_rn(g0, o.m[1])));
+                g = __fmaf_rn(bb0, o.m[5], __fmaf_rn(r0, o.m[3], __fmul_rn(g0, o.m[4])));
+                b = __fmaf_rn(bb0, o.m[8], __fmaf_rn(r0, o.m[6], __fmul_rn(g0, o.m[7])));
+            }
+            const size_t pi = size_t(Y) * o.w + X;
+            if (o.layout == PRR_PLANAR) {
+                o.r[pi] = r;
+                o.g[pi] = g;
+                o.b[pi] = b;
+            } else {
+                o.r[3 * pi] = r;
+                o.r[3 * pi + 1] = g;
+                o.r[3 * pi + 2] = b;
+            }
+        }
+}
+
+template <int CIN, int COUT, int MODE>
+__device__ __forceinline__ void epilogue(const ConvArgs& a, const RgbOut& o, TileCoord tc, uint32_t tmem,
+                                         const float* bias) {
     // A warp reads the 32 accumulator lanes of its quarter (the lanes tensor
     // memory lets it access), for two of the four blocks.
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, quarter = warp & 3;
@@ -321,13 +379,18 @@ __device__ __forceinline__ void epilogue(const ConvArgs& a, TileCoord tc, uint32
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if (py >= a.H || px >= a.W) continue;
         const bool keep = in_valid(a.valid, tc.img, px, py);
-        if (HEAD) {
-            float* o = a.yf + (size_t(tc.img) * kHead * a.H + py) * a.W + px;
+        if (MODE == kHeadRgb) {
+            float hv[COUT];
+#pragma unroll
+            for (int c = 0; c < COUT; c++) hv[c] = __fadd_rn(__uint_as_float(v[c]), bias[c]);
+            rgb_quad(o, px, py, a.W, a.H, hv);
+        } else if (MODE == kHeadF32) {
+            float* of = a.yf + (size_t(tc.img) * kHead * a.H + py) * a.W + px;
 #pragma unroll
             for (int c = 0; c < COUT; c++)
-                o[size_t(c) * a.H * a.W] = keep ? __fadd_rn(__uint_as_float(v[c]), bias[c]) : 0.0f;
+                of[size_t(c) * a.H * a.W] = keep ? __fadd_rn(__uint_as_float(v[c]), bias[c]) : 0.0f;
         } else {
-            uint4* o = a.y + (size_t(tc.img) * (COUT / 8) * a.H + py) * a.W + px;
+            uint4* oy = a.y + (size_t(tc.img) * (COUT / 8) * a.H + py) * a.W + px;
 #pragma unroll
             for (int c8 = 0; c8 < COUT / 8; c8++) {
                 float f[8];
@@ -336,16 +399,16 @@ __device__ __forceinline__ void epilogue(const ConvArgs& a, TileCoord tc, uint32
                     const float s = __fadd_rn(__uint_as_float(v[c8 * 8 + e]), bias[c8 * 8 + e]);
                     f[e] = keep ? fmaxf(s, 0.0f) : 0.0f;
                 }
-                o[size_t(c8) * a.H * a.W] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
-                                                       pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
+                oy[size_t(c8) * a.H * a.W] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
+                                                        pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
             }
         }
     }
 }
 
-template <int CIN, int COUT, bool HEAD>
+template <int CIN, int COUT, int MODE>
 __global__ void __launch_bounds__(kWsThreads) k_sg_conv(const __grid_constant__ CUtensorMap tmap, ConvArgs a,
-                                                         int tiles_x, int tiles_y, int ntiles) {
+                                                         RgbOut o, int tiles_x, int tiles_y, int ntiles) {
     using C = ConvCfg<CIN, COUT>;
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ __align__(8) uint64_t bars[2 * kStages + 2 * kAccs + 1];
@@ -440,7 +503,7 @@ __global__ void __launch_bounds__(kWsThreads) k_sg_conv(const __grid_constant__ 
                 break;
             }
             tc_fence_after();
-            epilogue<CIN, COUT, HEAD>(a, tile_coord(first + i * stride, tiles_x, tiles_y),
+            epilogue<CIN, COUT, MODE>(a, o, tile_coord(first + i * stride, tiles_x, tiles_y),
                                       tmem + uint32_t(q) * C::TMEM_COLS, bias_s);
             tc_fence_before();
             __syncwarp();
@@ -491,8 +554,8 @@ cudaError_t encode_window_map(CUtensorMap* map, const void* x, int c8, int H, in
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-template <int CIN, int COUT, bool HEAD>
-cudaError_t conv_launch(const ConvArgs& a, int images, cudaStream_t s) {
+template <int CIN, int COUT, int MODE>
+cudaError_t conv_launch(const ConvArgs& a, const RgbOut& o, int images, cudaStream_t s) {
     using C = ConvCfg<CIN, COUT>;
     // Weights and two window stages; at least 80 KB, so that no more than
     // two CTAs share an SM: two CTAs' 2 x 4 x COUT accumulator columns fit
@@ -500,7 +563,7 @@ cudaError_t conv_launch(const ConvArgs& a, int images, cudaStream_t s) {
     constexpr int smem = std::max(((C::W_BYTES + 127) & ~127) + kStages * ((C::WIN_BYTES + 127) & ~127), 80 * 1024);
     static int sms = 0;  // per process: the attribute and SM count of the first device used
     if (sms == 0) {
-        cudaError_t e = cudaFuncSetAttribute(k_sg_conv<CIN, COUT, HEAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(k_sg_conv<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              smem);
         if (e != cudaSuccess) return e;
         int dev = 0;
@@ -514,7 +577,7 @@ cudaError_t conv_launch(const ConvArgs& a, int images, cudaStream_t s) {
     const int tiles_x = (a.W + TX - 1) / TX, tiles_y = (a.H + TY - 1) / TY;
     const int ntiles = tiles_x * tiles_y * images;
     const int grid = std::max(1, std::min(ntiles, 2 * sms));
-    k_sg_conv<CIN, COUT, HEAD><<<grid, kWsThreads, smem, s>>>(map, a, tiles_x, tiles_y, ntiles);
+    k_sg_conv<CIN, COUT, MODE><<<grid, kWsThreads, smem, s>>>(map, a, o, tiles_x, tiles_y, ntiles);
     count_launch();
     return cudaGetLastError();
 }
@@ -604,49 +667,6 @@ __global__ void k_sg_pack_weights(const float* __restrict__ params, uint16_t* __
     const int kc = int((k / 8 / cout) % (cin / 8)), tap = int(k / 8 / cout / (cin / 8));
     const float wv = params[layer_off(l) + (size_t(n) * cin + kc * 8 + e) * 9 + tap];
     packed[i] = __bfloat16_as_ushort(__float2bfloat16_rn(wv));
-}
-
-struct OutArgs {
-    const float* head;  // [16][hq][wq], network frame
-    const float* base;  // [3][hq][wq], network frame
-    int w, h, wq, hq;
-    int rr, rc;         // mirrors of the network frame
-    int has_matrix;
-    float m[9];
-    int layout;
-    float* r;
-    float* g;
-    float* b;
-    const uint8_t* fallback;  // per 32x32 tile: developed by the plain kernel instead
-    int tiles_x;
-};
-
-__global__ void k_sg_output(OutArgs o) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= o.w) return;
-    if (o.fallback && o.fallback[(y / kDevelopTile) * o.tiles_x + x / kDevelopTile]) return;
-    const size_t plane = size_t(o.wq) * o.hq;
-    const size_t q = size_t(mirror_q(y >> 1, o.hq, o.rr)) * o.wq + mirror_q(x >> 1, o.wq, o.rc);
-    const int s = ((y & 1) ^ o.rr) * 2 + ((x & 1) ^ o.rc);
-    float r = fminf(__fadd_rn(o.head[(0 + s) * plane + q], o.base[q]), 1.0f);
-    float g = fminf(__fadd_rn(o.head[(4 + s) * plane + q], o.base[plane + q]), 1.0f);
-    float b = fminf(__fadd_rn(o.head[(8 + s) * plane + q], o.base[2 * plane + q]), 1.0f);
-    if (o.has_matrix) {
-        const float r0 = r, g0 = g, b0 = b;
-        r = __fmaf_rn(b0, o.m[2], __fmaf_rn(r0, o.m[0], __fmul_rn(g0, o.m[1])));
-        g = __fmaf_rn(b0, o.m[5], __fmaf_rn(r0, o.m[3], __fmul_rn(g0, o.m[4])));
-        b = __fmaf_rn(b0, o.m[8], __fmaf_rn(r0, o.m[6], __fmul_rn(g0, o.m[7])));
-    }
-    const size_t i = size_t(y) * o.w + x;
-    if (o.layout == PRR_PLANAR) {
-        o.r[i] = r;
-        o.g[i] = g;
-        o.b[i] = b;
-    } else {
-        o.r[3 * i] = r;
-        o.r[3 * i + 1] = g;
-        o.r[3 * i + 2] = b;
-    }
 }
 
 // Per 32x32 picture tile: does any quad's noise channel leave [lo, hi]?
@@ -889,8 +909,11 @@ struct NetBuffers {
     float* head = nullptr;    // [images][16][hq][wq]
 };
 
+// The seven layers; the head writes f32 channels (nb.head), or, given
+// `out`, the develop output directly.
 cudaError_t forward(const NetBuffers& nb, const uint16_t* packed, const float* params, const int4* valid, int images,
-                    int hq, int wq, unsigned* error, cudaStream_t s) {
+                    int hq, int wq, unsigned* error, cudaStream_t s, const RgbOut* out = nullptr) {
+    const RgbOut none{};
     ConvArgs a{};
     a.H = hq;
     a.W = wq;
@@ -903,14 +926,17 @@ cudaError_t forward(const NetBuffers& nb, const uint16_t* packed, const float* p
         cudaError_t e;
         if (l == 0) {
             a.y = nb.act[0];
-            e = conv_launch<kIn, kHid, false>(a, images, s);
+            e = conv_launch<kIn, kHid, kHidden>(a, none, images, s);
         } else if (l < kLayers - 1) {
             a.y = nb.act[l];
-            e = conv_launch<kHid, kHid, false>(a, images, s);
+            e = conv_launch<kHid, kHid, kHidden>(a, none, images, s);
+        } else if (out) {
+            a.y = nullptr;
+            e = conv_launch<kHid, kHead, kHeadRgb>(a, *out, images, s);
         } else {
             a.y = nullptr;
             a.yf = nb.head;
-            e = conv_launch<kHid, kHead, true>(a, images, s);
+            e = conv_launch<kHid, kHead, kHeadF32>(a, none, images, s);
         }
         if (e != cudaSuccess) return e;
     }
@@ -1073,10 +1099,11 @@ int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* param
     const size_t plane = size_t(wq) * hq;
     const int tiles_x = (d.w + kDevelopTile - 1) / kDevelopTile, tiles_y = (d.h + kDevelopTile - 1) / kDevelopTile;
     const size_t ntiles = size_t(tiles_x) * tiles_y;
-    // Scratch: input chunks, colours, two activation buffers, head, mask.
+    // Scratch: input chunks, colours, two activation buffers, mask (the head
+    // writes the output planes itself).
     const size_t o_in = 0, o_base = o_in + up256(plane * 32), o_a0 = o_base + up256(plane * 12),
-                 o_a1 = o_a0 + up256(plane * 64), o_head = o_a1 + up256(plane * 64),
-                 o_mask = o_head + up256(plane * 64), total = o_mask + up256(ntiles);
+                 o_a1 = o_a0 + up256(plane * 64), o_mask = o_a1 + up256(plane * 64),
+                 total = o_mask + up256(ntiles);
     PRR_TRY(c->cuda(L->scratch.ensure(total)));
     PRR_TRY(c->cuda(L->packed.ensure(sg::kPacked)));
     PRR_TRY(c->cuda(L->counters.ensure(2)));
@@ -1088,23 +1115,19 @@ int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* param
     uint4* a0 = reinterpret_cast<uint4*>(S + o_a0);
     uint4* a1 = reinterpret_cast<uint4*>(S + o_a1);
     for (int l = 0; l < 6; l++) nb.act[l] = (l & 1) ? a1 : a0;
-    nb.head = reinterpret_cast<float*>(S + o_head);
+    nb.head = nullptr;
     uint8_t* mask = S + o_mask;
     cudaStream_t s = c->stream;
     PRR_TRY(c->cuda(cudaMemsetAsync(L->counters.p, 0, 2 * sizeof(unsigned), s)));
     PRR_TRY(pack_frame(c, d, nb.in, base, nullptr));
     PRR_TRY(c->cuda(sg::pack_weights(model->dev_params, L->packed.p, s)));
-    PRR_TRY(c->cuda(sg::forward(nb, L->packed.p, model->dev_params, nullptr, 1, hq, wq, L->counters.p + 1, s)));
     sg::k_sg_fallback<<<unsigned(ntiles), 256, 0, s>>>(nb.in, wq, hq, d.cfa >> 1, d.cfa & 1, tiles_x, model->noise_lo,
                                                        model->noise_hi, mask, L->counters.p);
     count_launch();
-    sg::OutArgs o{};
-    o.head = nb.head;
+    sg::RgbOut o{};
     o.base = base;
     o.w = d.w;
     o.h = d.h;
-    o.wq = wq;
-    o.hq = hq;
     o.rr = d.cfa >> 1;
     o.rc = d.cfa & 1;
     o.has_matrix = d.has_matrix;
@@ -1115,8 +1138,7 @@ int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* param
     o.b = b;
     o.fallback = mask;
     o.tiles_x = tiles_x;
-    sg::k_sg_output<<<dim3((d.w + 255) / 256, d.h), 256, 0, s>>>(o);
-    count_launch();
+    PRR_TRY(c->cuda(sg::forward(nb, L->packed.p, model->dev_params, nullptr, 1, hq, wq, L->counters.p + 1, s, &o)));
     PRR_TRY(c->cuda(cudaGetLastError()));
     // The plain develop on the fallback tiles (the others return at once).
     d.tile_mask = mask;
