@@ -85,12 +85,19 @@ constexpr int WX = TX + 2, WY = TY + 2;  // input window
 constexpr int kConvThreads = 256;  // two warpgroups; each reads back two of a tile's four M blocks
 constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
 
+// The window is staged as two overlapping halves of HX columns (window
+// columns 0-17 and 16-33): M blocks 0-1 read the first, 2-3 the second. A
+// half's row of one chunk is 18 x 16 = 288 contiguous bytes in the
+// activation tensor, so each half is one TMA box with long rows.
+constexpr int HX = 18;
+
 template <int CIN, int COUT>
 struct ConvCfg {
     static constexpr int C8 = CIN / 8;
-    static constexpr int CS = WY * WX * 16;  // bytes per chunk plane of the window
-    static constexpr int RP = WX * 16;       // bytes per window row
-    static constexpr int WIN_BYTES = C8 * CS;
+    static constexpr int CS = WY * HX * 16;  // bytes per chunk plane of a half window
+    static constexpr int RP = HX * 16;       // bytes per half-window row
+    static constexpr int HALF_BYTES = C8 * CS;
+    static constexpr int WIN_BYTES = 2 * HALF_BYTES;
     static constexpr int W_BYTES = 9 * C8 * COUT * 16;
     static constexpr uint32_t TMEM_COLS = 4 * COUT;  // one tile's accumulators
     // Instruction descriptor, kind::f16: f32 accumulator (bits 4-5 = 1), A
@@ -242,8 +249,9 @@ __device__ __forceinline__ bool in_valid(const int4* valid, int b, int x, int y)
 // Warp-specialized and persistent. Each CTA walks tiles t = blockIdx.x,
 // + gridDim.x, ... with:
 //  - a producer warp: the layer's weights once (bulk copy), then each tile's
-//    input window by one TMA tensor load (box 8 x 34 x 18 x CIN/8 of the
-//    activation tensor, zero-filled outside the image) into a two-stage ring;
+//    input window by two TMA tensor loads (two halves of 18 x 18 pixels x
+//    CIN/8 chunks of the activation tensor, zero-filled outside the image)
+//    into a two-stage ring;
 //  - an MMA warp: per tile, 4 blocks x 9 taps x CIN/16 tcgen05.mma into one
 //    of two tensor-memory accumulators, then commits that free the window
 //    stage and publish the accumulator;
@@ -282,13 +290,15 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(bar) : "memory");
 }
 
-// One TMA tensor load of a window: coordinates (element, x, y, plane).
-__device__ __forceinline__ void tma_window(const CUtensorMap* map, uint32_t dst, uint32_t bar, int x, int y,
+// One TMA tensor load of a half window: coordinates (element along the
+// row = 8 x pixel, y, plane); the element coordinate is a multiple of 8
+// bf16 (16 bytes), negative at the left edge (zero fill).
+__device__ __forceinline__ void tma_window(const CUtensorMap* map, uint32_t dst, uint32_t bar, int xe, int y,
                                            int plane) {
     asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
         "[%2];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(0), "r"(x), "r"(y), "r"(plane)
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(xe), "r"(y), "r"(plane)
         : "memory");
 }
 
@@ -314,8 +324,10 @@ __device__ __forceinline__ void issue_tile(uint32_t win_a, uint32_t w_a, uint32_
 #pragma unroll
             for (int h = 0; h < C::C8 / 2; h++) {
                 // A: rows m = 8 * r + i are window pixel (r + dy, 8 bk + i + dx),
-                // K chunk k = the window's chunk plane 2 h + k.
-                const uint32_t aoff = uint32_t((2 * h) * C::CS + (t / 3) * C::RP + (8 * bk + t % 3) * 16) >> 4;
+                // i.e. column 8 (bk & 1) + i + dx of half bk >> 1; K chunk k =
+                // the half's chunk plane 2 h + k.
+                const uint32_t aoff = uint32_t((bk >> 1) * C::HALF_BYTES + (2 * h) * C::CS + (t / 3) * C::RP +
+                                               (8 * (bk & 1) + t % 3) * 16) >> 4;
                 // B: rows n = output channel, K chunk k = weights of input
                 // channels 16 h + 8 k .. + 7 at this tap.
                 const uint32_t boff = uint32_t((t * C::C8 + 2 * h) * COUT * 16) >> 4;
@@ -467,7 +479,9 @@ __global__ void __launch_bounds__(kWsThreads) k_sg_conv(const __grid_constant__ 
                 }
                 const TileCoord tc = tile_coord(first + i * stride, tiles_x, tiles_y);
                 mbar_expect_tx(full0 + 8 * s, uint32_t(C::WIN_BYTES));
-                tma_window(&tmap, win0 + uint32_t(s) * win_stride, full0 + 8 * s, tc.tx0 - 1, tc.ty0 - 1,
+                const uint32_t dst = win0 + uint32_t(s) * win_stride;
+                tma_window(&tmap, dst, full0 + 8 * s, 8 * (tc.tx0 - 1), tc.ty0 - 1, tc.img * C::C8);
+                tma_window(&tmap, dst + uint32_t(C::HALF_BYTES), full0 + 8 * s, 8 * (tc.tx0 + 15), tc.ty0 - 1,
                            tc.img * C::C8);
             }
         }
@@ -542,13 +556,14 @@ cudaError_t encode_window_map(CUtensorMap* map, const void* x, int c8, int H, in
         if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return e != cudaSuccess ? e : cudaErrorUnknown;
         fn = reinterpret_cast<EncodeTiledFn>(p);
     }
-    // The activation tensor as 4-D bf16: 8 channels of a chunk, x, y, and
-    // (image, chunk) planes; the window box covers one image's chunks.
-    const cuuint64_t dims[4] = {8, cuuint64_t(W), cuuint64_t(H), cuuint64_t(c8) * cuuint64_t(images)};
-    const cuuint64_t strides[3] = {16, cuuint64_t(W) * 16, cuuint64_t(W) * cuuint64_t(H) * 16};
-    const cuuint32_t box[4] = {8, WX, WY, cuuint32_t(c8)};
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box, estr,
+    // The activation tensor as 3-D bf16: a row of one chunk (8 channels x W
+    // pixels, contiguous), y, and (image, chunk) planes; the half-window box
+    // is HX pixels of a row, WY rows, one image's chunks.
+    const cuuint64_t dims[3] = {8 * cuuint64_t(W), cuuint64_t(H), cuuint64_t(c8) * cuuint64_t(images)};
+    const cuuint64_t strides[2] = {cuuint64_t(W) * 16, cuuint64_t(W) * cuuint64_t(H) * 16};
+    const cuuint32_t box[3] = {8 * HX, WY, cuuint32_t(c8)};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(x), dims, strides, box, estr,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
