@@ -577,7 +577,11 @@ constexpr uint32_t kIdFirstDc = 0, kIdDcReset = 1, kIdAcInitial = 8, kIdRnInitia
 // load replaces the arithmetic of the symbol loop's critical chain.
 struct EntropyTables {
     uint2 cw[kCodebooks * 32];  // x: base, y: length | sh1 << 8 | sh2 << 16
-    uint8_t ac[96], rn[32], ln[16], dc[16];  // next codebook index, by clamped symbol
+    // Next codebook indices after an AC symbol v, at [min(v, 94)]: AC table
+    // (bits 0-7, index min(v, 94)), LN (bits 8-15, min(v, 14)), RN (bits
+    // 16-23, min(v, 27)) -- one lookup for the three tables.
+    uint32_t nx[95];
+    uint8_t dc[16];  // next DC codebook index, by clamped magnitude
 };
 
 __device__ __forceinline__ void build_entropy_tables(EntropyTables& E, const CodeTables& T) {
@@ -604,32 +608,44 @@ __device__ __forceinline__ void build_entropy_tables(EntropyTables& E, const Cod
         }
         E.cw[i] = make_uint2(base, len | (sh1 << 8) | (sh2 << 16));
     }
-    for (uint32_t i = threadIdx.x; i < 95; i += blockDim.x) E.ac[i] = uint8_t(id_of(T.ac[i]));
-    for (uint32_t i = threadIdx.x; i < 28; i += blockDim.x) E.rn[i] = uint8_t(id_of(T.rn[i]));
-    for (uint32_t i = threadIdx.x; i < 15; i += blockDim.x) E.ln[i] = uint8_t(id_of(T.ln[i]));
+    for (uint32_t i = threadIdx.x; i < 95; i += blockDim.x)
+        E.nx[i] = id_of(T.ac[i]) | (id_of(T.ln[min(i, 14u)]) << 8) | (id_of(T.rn[min(i, 27u)]) << 16);
     for (uint32_t i = threadIdx.x; i < 13; i += blockDim.x) E.dc[i] = uint8_t(id_of(T.dc[i]));
 }
 
+// Big-endian words of the packet for the entropy kernel: from global memory
+// (swapped at load), or from the CTA's stage, swapped once when staged.
+// Both are indexed by the packet's word index.
+struct PacketWords {
+    const uint32_t* w;
+    __device__ __forceinline__ uint32_t be(uint32_t i) const { return bswap32(__ldg(w + i)); }
+};
+struct StagedWords {
+    const uint32_t* w;
+    uint32_t base;
+    __device__ __forceinline__ uint32_t be(uint32_t i) const { return w[i - base]; }
+};
+
 // The bit reader of src/bits.rs:17-112 with a refill that every lane runs
 // on every symbol, so that the refills of different lanes do not split the
-// warp. The word a refill would load is computed from the byte position
-// alone: n = min(4, end - pos) bytes at pos, big-endian, zero-filled, and pos
-// advances by n. That equals BitReader::next_word: whole words while four
-// bytes remain, then the partial tail, then zeros (pos is 4-aligned whenever
-// four bytes remain, so words_end need not be kept). It is ORed into the
-// window only when the count of bits below the view goes negative, exactly
-// as consume() does. Loads may touch the word after the stream's last byte,
-// which both word sources provide (padded packet, padded stage).
+// warp. BitReader::next_word returns whole aligned words while four bytes
+// remain, then the partial tail, then zeros: here the tail is read once at
+// set-up, so a refill is one aligned word (or the tail, or 0) selected by the
+// byte position. It is ORed into the window only when the count of bits
+// below the view goes negative, exactly as consume() does. Loads may touch
+// the word after the stream's last byte, which both word sources provide
+// (padded packet, padded stage).
 template <class Src>
 struct LeanReader {
     Src src;
-    uint32_t pos, end;
+    uint32_t pos, end, words_end, tail;
     uint64_t window;
     int32_t extra;
 
+    // n = min(4, end - p) bytes at byte p, big-endian, zero-filled (set-up only).
     __device__ __forceinline__ uint32_t word_at(uint32_t p) const {
         const uint32_t k = p >> 2;
-        const uint32_t hi = bswap32(src(k)), lo = bswap32(src(k + 1));
+        const uint32_t hi = src.be(k), lo = src.be(k + 1);
         const uint32_t w = __funnelshift_l(lo, hi, (p & 3) * 8);
         const uint32_t n = min(4u, end - min(p, end));
         return n == 0 ? 0u : (w & (0xFFFFFFFFu << (32 - 8 * n)));
@@ -650,8 +666,13 @@ struct LeanReader {
         if (to_boundary != 0 && to_boundary <= remaining) {
             low = word_at(pos) & (0xFFFFFFFFu << (32 - 8 * to_boundary));
             pos += to_boundary;
+            remaining -= to_boundary;
             extra = int32_t(8 * to_boundary);
         }
+        // Whole words while pos < words_end (pos is then 4-aligned), then
+        // the tail of end - words_end < 4 bytes, then zeros.
+        words_end = pos + 4 * (remaining / 4);
+        tail = word_at(words_end);
         window = (uint64_t(first) << 32) | uint64_t(low);
     }
 
@@ -659,13 +680,15 @@ struct LeanReader {
 
     // BitReader::consume (src/bits.rs:348-356).
     __device__ __forceinline__ void consume(uint32_t n) {
-        const uint32_t w = word_at(pos);  // independent of n: issued early
+        const bool whole = pos < words_end;
+        const uint32_t ww = src.be(pos >> 2);  // independent of n: issued early
+        const uint32_t w = whole ? ww : (pos < end ? tail : 0u);
+        const uint32_t adv = whole ? 4u : end - pos;
         window <<= (n & 63);
         extra = int32_t(uint32_t(extra) - n);
         const bool refill = extra < 0;
         const uint32_t shift = uint32_t(-int32_t(int8_t(extra))) & 63;
         window |= refill ? (uint64_t(w) << shift) : 0ull;
-        const uint32_t adv = min(4u, end - min(pos, end));
         pos += refill ? adv : 0u;
         extra += refill ? 32 : 0;
     }
@@ -745,9 +768,8 @@ __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off,
         const bool is_level = state >= LEVELS;
         const bool negative = int32_t(top << (l & 31)) < 0;
         r.consume(l + (is_level ? 1u : 0u));
-        const uint32_t ac_next = T.ac[min(v, 94u)];
-        const uint32_t ln_next = T.ln[min(v, 14u)];
-        const uint32_t rn_next = T.rn[min(v, 27u)];
+        const uint32_t nx = T.nx[min(v, 94u)];
+        const uint32_t ac_next = nx & 0xFF, ln_next = (nx >> 8) & 0xFF, rn_next = nx >> 16;
         if (is_level) {
             const uint32_t mag = (v + 1) & 0xFFFF;
             if (cnt < codes) append(n, negative ? (0u - mag) : mag);
@@ -797,7 +819,10 @@ __device__ __forceinline__ void entropy_chunk(const EntropyTables& T, uint32_t* 
     if (staged) {
         const uint4* src = reinterpret_cast<const uint4*>(d.words) + base / 16;
         uint4* dst = reinterpret_cast<uint4*>(stage);
-        for (uint32_t i = threadIdx.x; i < (top - base) / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+        for (uint32_t i = threadIdx.x; i < (top - base) / 16; i += blockDim.x) {
+            const uint4 v = __ldg(src + i);
+            dst[i] = make_uint4(bswap32(v.x), bswap32(v.y), bswap32(v.z), bswap32(v.w));
+        }
     }
     __syncthreads();
     const uint32_t g = chunk * blockDim.x + threadIdx.x;
@@ -820,8 +845,8 @@ __device__ __forceinline__ void entropy_chunk(const EntropyTables& T, uint32_t* 
     uint32_t* list = d.pairs + stream_list_base(d, trow, x, log2, s, LC);
     bool revisited = false, ok = true;
     const uint32_t cnt =
-        staged ? entropy_events<LC>(SharedWords{stage, base >> 2}, soff, slen, log2, T, list, revisited, ok)
-               : entropy_events<LC>(GlobalWords{d.words}, soff, slen, log2, T, list, revisited, ok);
+        staged ? entropy_events<LC>(StagedWords{stage, base >> 2}, soff, slen, log2, T, list, revisited, ok)
+               : entropy_events<LC>(PacketWords{d.words}, soff, slen, log2, T, list, revisited, ok);
     if (!ok) atomicOr(&st->error, 1u);
     d.counts[g] = revisited ? 0x80000000u : cnt;
 }
