@@ -565,6 +565,188 @@ def run_batch_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# Clip workload: a QuickTime movie of 5760x3040 frames (the headline frames,
+# CLIP_DISTINCT distinct packets repeated to CLIP_N samples, 4 samples to a
+# chunk) written to the local temp directory, so it sits in the page cache,
+# and decoded by the clip pipeline: reader threads read samples into pinned
+# memory while the device decodes the previous batch. One step = one pass
+# over the whole clip. value: frames over the summed device time of the
+# batch kernels; e2e: frames over the wall time of the pass (reads, uploads,
+# kernels, statuses back), the frames left decoded in HBM. The batches of
+# the two lanes overlap on the device; each counts the part of its kernel
+# interval after the previous batch's kernels ended. The sequential
+# loop a crate caller writes (read one sample, decode it) is timed beside it
+# through the library's host-buffer decode call.
+
+CLIP_N, CLIP_DISTINCT, CLIP_BATCH, CLIP_THREADS = 96, 4, 16, 16
+CLIP_METRIC = "clip decode frames/s (movie file -> decoded 5.8K frames in HBM, bit-exact)"
+
+
+def clip_file(n_frames):
+    import tempfile
+
+    from proresraw_rs_b200 import synth_movie as M
+
+    pkts = make_packets(CLIP_DISTINCT)
+    path = os.path.join(tempfile.gettempdir(), f"prr_clip_{os.getpid()}.mov")
+    M.write_clip(path, [pkts[i % CLIP_DISTINCT] for i in range(n_frames)], per_chunk=4, make="synthetic")
+    return path, pkts
+
+
+def clip_cpu(track, budget_s: float):
+    """The oracle on the host cores: read a sample, decode it (all threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+
+    threads = os.cpu_count() or 1
+    O.decode_frame(track.sample(0), 0, threads)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        O.decode_frame(track.sample(n % len(track.samples)), 0, threads)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or n >= 20 * len(track.samples):
+            break
+    return n / el, n, el, threads
+
+
+def run_clip(args):
+    import torch
+
+    import proresraw_rs_b200 as P
+    from proresraw_rs_b200 import _lib
+    from proresraw_rs_b200 import clip as CL
+    from proresraw_rs_b200 import mov
+
+    world, rank, local = dist_setup(args.gpus)
+    L = _lib.lib()
+    path, pkts = clip_file(args.clip_frames)
+    try:
+        track = mov.read_video_track(path)
+        nf = len(track.samples)
+        dec = CL.ClipDecoder(track, args.clip_batch, args.clip_threads)
+
+        def one_pass(check=False):
+            frames, dev_ms = 0, 0.0
+            for batch in dec.batches():
+                if check:
+                    assert not any(isinstance(f, Exception) for f in batch.frames)
+                frames += len(batch.frames)
+                dev_ms += batch.busy_ms
+            return frames, dev_ms
+
+        assert one_pass(check=True)[0] == nf
+        for _ in range(max(3, args.warmup)):
+            one_pass()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        launches0 = L.prr_kernel_launches()
+        dev_total = 0.0
+        with Clocks(torch.cuda.current_device()) as clocks:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                dev_total += one_pass()[1]
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+        launches = L.prr_kernel_launches() - launches0
+        t = torch.tensor([dev_total, wall], dtype=torch.float64, device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max, wall_max = float(t[0].item()), float(t[1].item())
+        # The sequential loop: read one sample, decode it from the host buffer.
+        seq_n = min(nf, 48)
+        ctx = P.context()
+        info = P.frame_info(pkts[0])
+        out = torch.empty(info.coded_width * info.coded_height, dtype=torch.uint16, device="cuda")
+        res, err = _lib.CDecodeResult(), _lib.CError()
+        buf = bytearray(max(s.size for s in track.samples))
+        cbuf = (C.c_uint8 * len(buf)).from_buffer(buf)
+        for _ in range(2):
+            track.read_at(track.samples[0].offset, memoryview(buf)[:track.samples[0].size])
+            L.prr_decode(ctx, C.addressof(cbuf), track.samples[0].size, 0, out.data_ptr(), out.numel(),
+                         C.byref(res), C.byref(err))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for i in range(seq_n):
+            s = track.samples[i]
+            track.read_at(s.offset, memoryview(buf)[:s.size])
+            rc = L.prr_decode(ctx, C.addressof(cbuf), s.size, 0, out.data_ptr(), out.numel(), C.byref(res),
+                              C.byref(err))
+            assert rc == 0
+        seq_fps = seq_n / (time.perf_counter() - t1)
+        if rank == 0:
+            peak, peak_kind = peaks()
+            cw, ch = info.coded_width, info.coded_height
+            alg = sum(s.size for s in track.samples) + 2 * cw * ch * nf
+            achieved = alg / (ms_max / args.steps / 1000.0) / 1e9
+            h2d = sum(s.size for s in track.samples)
+            line = {
+                "metric": CLIP_METRIC, "value": world * args.steps * nf / (ms_max / 1000.0), "unit": "frames/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+                "config": {"workload": f"QuickTime clip of {nf} samples ({CLIP_DISTINCT} distinct {W}x{H} BGGR v0 "
+                                       "align4 qscale45 packets, 0.5% corrupt tiles), file in the page cache; "
+                                       "decode_frame (Apple) of every sample",
+                           "frames_per_step": nf, "frames_per_batch": args.clip_batch,
+                           "reader_threads": args.clip_threads, "clip_bytes": os.path.getsize(path),
+                           "l2": f"{2 * cw * ch * nf / 1e9:.1f} GB of code values written per pass, more than L2",
+                           "parallelism": f"replicas x{world}",
+                           "sequential_read_then_decode_fps": seq_fps},
+                "roofline": {"bound": "hbm", "kernel": "k_batch_decode", "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                             "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg},
+                "gpu_launches": int(launches),
+                "e2e": {"value": world * args.steps * nf / wall_max, "unit": "frames/s",
+                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 16 * nf,
+                        "note": "ClipDecoder.batches over the movie file: positional reads into pinned memory, "
+                                "uploads, kernels, statuses back; frames stay on the device"},
+            }
+            cl = clocks.summary()
+            if cl:
+                line["clocks"] = cl
+            if world == 1 and not args.no_cpu_baseline:
+                v, n, el, threads = clip_cpu(track, 12.0)
+                line["cpu_baseline"] = {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+                                        "sample": f"{n} samples read from the clip and decoded by the oracle, "
+                                                  f"{threads} threads, {el:.1f} s"}
+            print(json.dumps(line), flush=True)
+        dec.close()
+        track.close()
+    finally:
+        os.remove(path)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_clip_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    from proresraw_rs_b200 import mov
+
+    path, _ = clip_file(args.clip_frames)
+    try:
+        with mov.read_video_track(path) as track:
+            v, n, el, threads = clip_cpu(track, max(10.0, 0.5 * args.steps))
+    finally:
+        os.remove(path)
+    line = {
+        "impl": "reference", "metric": CLIP_METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / n * args.clip_frames,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": f"QuickTime clip of {args.clip_frames} {W}x{H} samples; read_at + decode_frame",
+                   "frames_per_step": args.clip_frames},
+        "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} samples read and decoded by the CPU oracle, {threads} threads, {el:.1f} s"},
+        "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
 # Learned develop workloads. The surrogate is trained here, on the device,
 # by the library's own kernels: 4000 random 512x512 crops of synthetic
 # 4096x2160 RGGB frames (the mosaic generator with noise sigma uniform in
@@ -882,20 +1064,26 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="5k8", choices=["5k8", "mixed-batch", "learned", "8k-stream"],
+    ap.add_argument("--workload", default="5k8", choices=["5k8", "mixed-batch", "learned", "8k-stream", "clip"],
                     help="5k8: the headline single-frame decode+develop; mixed-batch: 64 uneven frames per step; "
-                         "learned: surrogate develop of 4K frames (trains first); 8k-stream: 16 8K frames per step")
+                         "learned: surrogate develop of 4K frames (trains first); 8k-stream: 16 8K frames per step; "
+                         "clip: a movie file of 5.8K frames through the clip pipeline, one pass per step")
     ap.add_argument("--epochs", type=int, default=8, help="training epochs for the learned workloads")
     ap.add_argument("--save-model", default="", help="learned: save the trained surrogate (.npz)")
     ap.add_argument("--model", default=os.path.join(ROOT, "proresraw_rs_b200", "data", "surrogate.npz"),
                     help="8k-stream: a trained surrogate (.npz; default the packaged one); trained here if absent")
     ap.add_argument("--batch-frames", type=int, default=BATCH_N, help="mixed-batch: frames per batch")
     ap.add_argument("--no-tune", action="store_true", help="mixed-batch: skip the autotuner (default shape)")
+    ap.add_argument("--clip-frames", type=int, default=CLIP_N, help="clip: samples in the movie")
+    ap.add_argument("--clip-batch", type=int, default=CLIP_BATCH, help="clip: frames per batch")
+    ap.add_argument("--clip-threads", type=int, default=CLIP_THREADS, help="clip: reader threads")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     args = ap.parse_args()
     if args.workload == "mixed-batch":
         return run_batch_reference(args) if args.impl == "reference" else run_batch(args)
+    if args.workload == "clip":
+        return run_clip_reference(args) if args.impl == "reference" else run_clip(args)
     if args.workload in ("learned", "8k-stream"):
         if args.impl == "reference":
             return run_reference(args)

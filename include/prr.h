@@ -51,6 +51,7 @@ enum prr_status {
     PRR_ERR_INVALID = -23, /* an argument is out of range */
     PRR_ERR_NO_MEMORY = -24,
     PRR_ERR_SCRATCH_LIMIT = -25, /* the frame has more tiles than prr_decode_noalloc's fixed scratch holds */
+    PRR_ERR_MOVIE = -26,         /* a movie could not be read (mov::Error); the message says why */
 };
 
 /* Largest tile count prr_decode_noalloc accepts (8192x4320 at alignment 0
@@ -359,6 +360,101 @@ int prr_sg_gradients(prr_ctx* ctx, const float* in16, const float* base3, const 
 int prr_decode_develop_host(prr_ctx* ctx, const uint8_t* packet, size_t len, int idct,
                             const prr_params* params, int stage, int layout, float* r, float* g,
                             float* b, size_t out_len, prr_decode_result* res, prr_error* err);
+
+/* --- movie sample tables (src/mov.rs) ------------------------------------------ */
+/* The first enabled video track of a QuickTime / ISO movie: the samples it
+ * presents (after the first non-empty edit), its rate and the movie's text
+ * metadata. Host code; only the `moov` atom is read into memory. A track
+ * keeps the file open for prr_mov_read_at (positional reads, safe from any
+ * number of threads at once). */
+typedef struct prr_mov_track prr_mov_track;
+
+/* The sample description's fourcc filter, `accept: fn(&[u8; 4]) -> bool`
+ * (src/mov.rs:173). Non-zero accepts. */
+typedef int (*prr_mov_accept_fn)(const uint8_t fourcc[4], void* user);
+
+/* mov::Sample (src/mov.rs:91-98). */
+typedef struct prr_mov_sample {
+    uint64_t offset; /* byte offset of the sample in the file */
+    uint32_t size;   /* the sample's length in bytes */
+    uint32_t pad;
+} prr_mov_sample;
+
+/* mov::Track without its vectors (src/mov.rs:100-124). orientation is the
+ * EXIF value 1..8 (Orientation::exif, src/mov.rs:150-157). */
+typedef struct prr_mov_info {
+    uint8_t fourcc[4];
+    uint32_t fps_num, fps_den;
+    uint8_t variable_durations;
+    uint8_t orientation;
+    uint8_t has_creation_time;
+    uint8_t reserved;
+    uint64_t creation_time; /* seconds since 1904-01-01 UTC (mvhd), when has_creation_time */
+    uint64_t n_samples;
+    uint32_t n_warnings;
+    uint32_t n_metadata;
+} prr_mov_info;
+
+/* mov::read_video_track (src/mov.rs:172-177) on the file at path. accept
+ * NULL: is_prores_raw_fourcc (src/lib.rs:72-75). On failure returns
+ * PRR_ERR_MOVIE with the crate's message in msg (truncated to msg_cap). */
+int prr_mov_open(const char* path, prr_mov_accept_fn accept, void* user, prr_mov_track** out, char* msg,
+                 size_t msg_cap);
+void prr_mov_close(prr_mov_track* track);
+int prr_mov_get_info(const prr_mov_track* track, prr_mov_info* info);
+/* Track::samples[first .. first + count]. */
+int prr_mov_get_samples(const prr_mov_track* track, size_t first, size_t count, prr_mov_sample* out);
+/* Track::warnings[i]; NULL past the end. Owned by the track. */
+const char* prr_mov_warning(const prr_mov_track* track, size_t i);
+/* Track::metadata[i] as UTF-8 key and value, owned by the track. */
+int prr_mov_metadata(const prr_mov_track* track, size_t i, const char** key, const char** value);
+/* mov::read_at (src/mov.rs:179-183): len bytes at offset of the track's file. */
+int prr_mov_read_at(const prr_mov_track* track, uint64_t offset, uint8_t* buf, size_t len, char* msg,
+                    size_t msg_cap);
+
+/* --- clip pipeline: a movie's frames through the batch decoder --------------- */
+/* The frames of a movie track decoded batch by batch, the host's reads and
+ * uploads overlapping the device's decode. No single counterpart in the
+ * crate: each frame is mov::read_at (src/mov.rs:179-183) then
+ * decode_frame_with / decode_frame_reduced_with (src/decoder.rs:226-267,
+ * src/reduced.rs:147-201), with their outputs and errors. While the device
+ * decodes batch k, batch k+1 is uploaded and queued on a second stream and
+ * reader threads read batch k+2's samples straight into pinned memory. */
+typedef struct prr_clip prr_clip;
+typedef struct prr_clip_batch {
+    uint64_t first;    /* track sample index of the batch's first frame */
+    uint32_t n;        /* frames in the batch; 0 past the end of the range */
+    float device_ms;   /* device time of the batch's kernels */
+    float busy_ms;     /* the part of device_ms after the previous batch's kernels
+                          ended: summed over a range, the device's busy time */
+    uint32_t pad;
+    prr_job* jobs;     /* n jobs, owned by the clip: each frame's status, result
+                          (header, max_qscale, skipped tiles), error and device
+                          output (dev_out, out_len); PRR_ERR_MOVIE when its
+                          sample could not be read (prr_clip_last_error) */
+    void* cuda_stream; /* the cudaStream_t the batch was decoded on */
+} prr_clip_batch;
+
+/* A pipeline over `track` (which must stay open): frames_per_batch frames a
+ * batch, reader_threads host threads for the reads. */
+int prr_clip_create(int device, const prr_mov_track* track, uint32_t frames_per_batch, uint32_t reader_threads,
+                    prr_clip** out);
+/* The same over a caller's own sample table (mov::Track::samples) and open
+ * file descriptor (the movie's File, which must stay open), for callers
+ * with their own movie reader. */
+int prr_clip_create_fd(int device, int fd, const prr_mov_sample* samples, size_t n_samples,
+                       uint32_t frames_per_batch, uint32_t reader_threads, prr_clip** out);
+void prr_clip_destroy(prr_clip* clip);
+/* Begin decoding samples [first, first + count) at `scale` (PRR_SCALE_FULL
+ * with `idct`, or a prr_scale with `greens`); ends any range in progress. */
+int prr_clip_start(prr_clip* clip, uint64_t first, uint64_t count, int scale, int idct, int greens);
+/* The next decoded batch, in order (n = 0 at the end). Its outputs stay valid
+ * until the next call; work reading them must be enqueued on cuda_stream,
+ * which orders it before the buffers are reused, or be complete by then.
+ * An error status ends the range (start again). */
+int prr_clip_next(prr_clip* clip, prr_clip_batch* out);
+/* The message of the last failed read or call. */
+const char* prr_clip_last_error(const prr_clip* clip);
 
 /* --- diagnostics -------------------------------------------------------------- */
 /* The device inverse transforms on raw blocks (idct.rs): kind 0 Apple 8x8,

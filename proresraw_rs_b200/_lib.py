@@ -29,6 +29,7 @@ ERR_TIMEOUT = -22
 ERR_INVALID = -23
 ERR_NO_MEMORY = -24
 ERR_SCRATCH_LIMIT = -25
+ERR_MOVIE = -26
 NOALLOC_MAX_TILES = 262144
 
 
@@ -149,6 +150,44 @@ class CSgModel(C.Structure):
     ]
 
 
+class CMovSample(C.Structure):
+    _fields_ = [
+        ("offset", C.c_uint64),
+        ("size", C.c_uint32),
+        ("pad", C.c_uint32),
+    ]
+
+
+class CMovInfo(C.Structure):
+    _fields_ = [
+        ("fourcc", C.c_uint8 * 4),
+        ("fps_num", C.c_uint32),
+        ("fps_den", C.c_uint32),
+        ("variable_durations", C.c_uint8),
+        ("orientation", C.c_uint8),
+        ("has_creation_time", C.c_uint8),
+        ("reserved", C.c_uint8),
+        ("creation_time", C.c_uint64),
+        ("n_samples", C.c_uint64),
+        ("n_warnings", C.c_uint32),
+        ("n_metadata", C.c_uint32),
+    ]
+
+
+MOV_ACCEPT_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_uint8), C.c_void_p)
+
+
+class CClipBatch(C.Structure):
+    _fields_ = [
+        ("first", C.c_uint64),
+        ("n", C.c_uint32),
+        ("device_ms", C.c_float),
+        ("busy_ms", C.c_float),
+        ("pad", C.c_uint32),
+        ("jobs", C.POINTER(CJob)),
+        ("cuda_stream", C.c_void_p),
+    ]
+
 SCALE_FULL = 0
 
 _lib = None
@@ -220,6 +259,19 @@ def lib():
         "prr_sg_trainer_device_params": (vp, [vp]),
         "prr_sg_trainer_step": (i, [vp, vp, C.c_float, P(C.c_float)]),
         "prr_sg_gradients": (i, [vp, vp, vp, vp, C.c_uint32, C.c_uint32, vp, vp, vp, P(C.c_double)]),
+        "prr_mov_open": (i, [C.c_char_p, MOV_ACCEPT_FN, vp, P(vp), C.c_char_p, sz]),
+        "prr_mov_close": (None, [vp]),
+        "prr_mov_get_info": (i, [vp, P(CMovInfo)]),
+        "prr_mov_get_samples": (i, [vp, sz, sz, P(CMovSample)]),
+        "prr_mov_warning": (C.c_char_p, [vp, sz]),
+        "prr_mov_metadata": (i, [vp, sz, P(C.c_char_p), P(C.c_char_p)]),
+        "prr_mov_read_at": (i, [vp, C.c_uint64, vp, sz, C.c_char_p, sz]),
+        "prr_clip_create": (i, [i, vp, C.c_uint32, C.c_uint32, P(vp)]),
+        "prr_clip_create_fd": (i, [i, i, P(CMovSample), sz, C.c_uint32, C.c_uint32, P(vp)]),
+        "prr_clip_destroy": (None, [vp]),
+        "prr_clip_start": (i, [vp, C.c_uint64, C.c_uint64, i, i, i]),
+        "prr_clip_next": (i, [vp, P(CClipBatch)]),
+        "prr_clip_last_error": (C.c_char_p, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -1,6 +1,7 @@
 """Builds the package's native libraries in-tree.
 
  - lib/libprr.so        CUDA sm_100a kernels + the C ABI of include/prr.h
+                        (and the host movie reader)
  - lib/libprr_synth.so  host C++ synthetic-input generator and encoder
 
 Float flags matter for bit-exactness: -fmad=false (the device code spells
@@ -29,7 +30,9 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O3",
     "-shared",
 ]
-CUDA_SOURCES = ["api.cu", "batch.cu", "decode.cu", "develop.cu", "learned.cu", "noalloc.cu"]
+CUDA_SOURCES = ["api.cu", "batch.cu", "clip.cu", "decode.cu", "develop.cu", "learned.cu", "noalloc.cu"]
+# Host-only parts of libprr.so (the movie reader); nvcc hands them to g++.
+HOST_SOURCES = ["mov.cpp"]
 CXX_FLAGS = ["-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-shared"]
 
 
@@ -63,7 +66,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     os.makedirs(LIB, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers += [os.path.join(HERE, "..", "include", "prr.h"), os.path.join(HERE, "..", "include", "prr_synth.h")]
-    cu = [os.path.join(CSRC, f) for f in CUDA_SOURCES]
+    cu = [os.path.join(CSRC, f) for f in CUDA_SOURCES + HOST_SOURCES]
     out = os.path.join(LIB, "libprr.so")
     if force or _stale(out, cu + headers):
         cmd = [nvcc(), *NVCC_FLAGS, *(["-Xptxas", "-v"] if ptxas_info else []), "-o", out, *cu]

@@ -269,14 +269,31 @@ int enqueue_kernels(prr_ctx* c, BatchState* B, Bucket& bk, const prr_batch_confi
     return c->cuda(cudaGraphLaunch(bk.exec, c->stream));
 }
 
-int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force) {
+// `staged`: the jobs' packets already lie in this pinned host buffer of
+// `staged_bytes`, each at a 16-byte aligned offset with its padded length
+// inside the buffer; the buffer is uploaded as it is, without the copy into
+// the batch's own staging. It must stay unchanged until the batch is waited
+// for.
+int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force, const uint8_t* staged = nullptr,
+           size_t staged_bytes = 0) {
     if (!c || (!jobs && n > 0)) return PRR_ERR_INVALID;
     PRR_TRY(c->use_device());
     BatchState* B = nullptr;
     PRR_TRY(batch_state(c, &B));
     if (B->pending) return PRR_ERR_INVALID;  // wait for the previous batch first
-    const Totals t = plan_batch(jobs, n, B->plan);
+    Totals t = plan_batch(jobs, n, B->plan);
     const size_t nf = B->plan.size();
+    if (staged) {
+        for (FramePlan& f : B->plan) {
+            const prr_job& j = jobs[f.job];
+            const uint8_t* p = j.packet;
+            if (p < staged || (p - staged) % 16 != 0 ||
+                size_t(p - staged) + up16(prr_padded_packet_bytes(size_t(j.len))) > staged_bytes)
+                return PRR_ERR_INVALID;
+            f.pkt_off = size_t(p - staged);
+        }
+        t.packet_bytes = staged_bytes;
+    }
     B->jobs = jobs;
     B->njobs = n;
     if (nf == 0) {
@@ -304,7 +321,7 @@ int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force) {
     PRR_TRY(c->cuda(B->grow(B->pairs, std::max<size_t>(t.pairs, 64))));
     PRR_TRY(c->cuda(B->grow(B->status, grid_frames)));
     PRR_TRY(c->cuda(B->hmeta.ensure(meta_bytes)));
-    PRR_TRY(c->cuda(B->hpackets.ensure(t.packet_bytes)));
+    if (!staged) PRR_TRY(c->cuda(B->hpackets.ensure(t.packet_bytes)));
     PRR_TRY(c->cuda(B->grow(B->hstatus, grid_frames)));
     int max_per_sm = 0;
     PRR_TRY(c->cuda(batch_max_ctas_per_sm(cfg.stage_bytes, &max_per_sm)));
@@ -325,7 +342,7 @@ int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force) {
     for (size_t i = 0; i < nf; i++) {
         const FramePlan& f = B->plan[i];
         const prr_job& j = jobs[f.job];
-        std::memcpy(B->hpackets.p + f.pkt_off, j.packet, size_t(j.len));
+        if (!staged) std::memcpy(B->hpackets.p + f.pkt_off, j.packet, size_t(j.len));
         BatchFrame& F = hf[i];
         std::memset(&F, 0, sizeof(F));
         F.d = make_frame_desc(f.info, B->packets.p + f.pkt_off);
@@ -348,8 +365,8 @@ int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force) {
     }
     PRR_TRY(c->cuda(cudaMemcpyAsync(B->meta.p, B->hmeta.p, sizeof(BatchHeader) + nf * sizeof(BatchFrame),
                                     cudaMemcpyHostToDevice, c->stream)));
-    PRR_TRY(c->cuda(cudaMemcpyAsync(B->packets.p, B->hpackets.p, t.packet_bytes, cudaMemcpyHostToDevice,
-                                    c->stream)));
+    PRR_TRY(c->cuda(cudaMemcpyAsync(B->packets.p, staged ? staged : B->hpackets.p, t.packet_bytes,
+                                    cudaMemcpyHostToDevice, c->stream)));
     BatchDesc desc{};
     desc.hdr = reinterpret_cast<const BatchHeader*>(B->meta.p);
     desc.frames = reinterpret_cast<const BatchFrame*>(B->meta.p + sizeof(BatchHeader));
@@ -416,6 +433,16 @@ int wait(prr_ctx* c, uint32_t timeout_ms) {
 }
 
 }  // namespace
+
+int batch_submit_staged(prr_ctx* c, prr_job* jobs, size_t n, const uint8_t* staged, size_t staged_bytes) {
+    if (!staged) return PRR_ERR_INVALID;
+    return submit(c, jobs, n, nullptr, staged, staged_bytes);
+}
+int batch_wait(prr_ctx* c, uint32_t timeout_ms) { return wait(c, timeout_ms); }
+float batch_last_ms(prr_ctx* c) { return c && c->batch ? c->batch->last_ms : 0.f; }
+cudaEvent_t batch_start_event(prr_ctx* c) { return c && c->batch ? c->batch->ev_start : nullptr; }
+cudaEvent_t batch_stop_event(prr_ctx* c) { return c && c->batch ? c->batch->ev_stop : nullptr; }
+
 }  // namespace prr
 
 using namespace prr;
