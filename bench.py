@@ -86,14 +86,42 @@ def traffic_from_profiles():
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """SM clocks and clock-event reasons during the timed region: read through
+    NVML every 10 ms on a thread (short timed regions get samples too), with
+    `nvidia-smi -lms 200` beside it; reading only."""
+
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.samples = []  # (sm_mhz, max_mhz, reasons)
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _nvml_loop(self):
+        try:
+            import pynvml as N
+
+            N.nvmlInit()
+            h = N.nvmlDeviceGetHandleByIndex(self.index)
+            bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
+                    N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]
+            mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+            while True:
+                sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(mx), [n for n, b in zip(self.NAMES, bits) if r & b]))
+                if self._stop.wait(0.01):
+                    break
+            N.nvmlShutdown()
+        except Exception:
+            pass
 
     def __enter__(self):
+        self._thread = threading.Thread(target=self._nvml_loop, daemon=True)
+        self._thread.start()
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
@@ -109,6 +137,9 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -118,18 +149,25 @@ class Clocks:
             self.f.close()
 
     def summary(self):
+        sm, mx, reasons = [], [], set()
+        for s_mhz, m_mhz, rs in self.samples:
+            sm.append(s_mhz)
+            mx.append(m_mhz)
+            reasons.update(rs)
         try:
             rows = [l.strip().split(", ") for l in open(self.path) if l.strip()]
         except OSError:
+            rows = []
+        for r in rows:
+            if len(r) > 2 and r[1].replace(".", "").isdigit():
+                sm.append(float(r[1]))
+            if len(r) > 2 and r[2].replace(".", "").isdigit():
+                mx.append(float(r[2]))
+            reasons.update(self.NAMES[i] for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active")
+        if not sm:
             return None
-        if not rows:
-            return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
 
 
 def cpu_baseline(pkts, budget_s: float = 15.0):
@@ -747,6 +785,227 @@ def run_clip_reference(args):
 
 
 # ---------------------------------------------------------------------------
+# DNG workload: the headline 5760x3040 frames exported as the crate's DNG
+# files (code values + LinearizationTable, 256-square lossless JPEG tiles).
+# One step = one frame. value: frames over the device time of the decode and
+# the tile encoder with packets resident in HBM; e2e: frames over the wall
+# time of prr_decode (host packet) + prr_dng_write (tiles encoded on the
+# device, brought back, the TIFF container written on the host), the file's
+# bytes in host memory, on several host threads.
+
+DNG_METRIC = "5.8K frames/s decode + DNG export (lossless JPEG tiles, bit-exact)"
+
+
+def dng_cpu(pkts, budget_s: float):
+    """The oracle on the host cores: decode, cut and encode every tile."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+
+    threads = os.cpu_count() or 1
+    f = O.decode_frame(pkts[0], 0, threads)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        f = O.decode_frame(pkts[n % len(pkts)], 0, threads)
+        O.lj92_tiles(f.samples, W, H, stride=f.header.coded_width, threads=threads)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or n >= 200:
+            break
+    return n / el, n, el, threads
+
+
+def run_dng(args):
+    import torch
+
+    import proresraw_rs_b200 as P
+    from proresraw_rs_b200 import _lib
+
+    world, rank, local = dist_setup(args.gpus)
+    L = _lib.lib()
+    pkts = make_packets(RING)
+    infos = [P.frame_info(p) for p in pkts]
+    info0 = infos[0]
+    s = torch.cuda.Stream()
+    ctx = C.c_void_p()
+    assert L.prr_ctx_create(torch.cuda.current_device(), C.c_void_p(s.cuda_stream), C.byref(ctx)) == 0
+    dpk = []
+    for p in pkts:
+        buf = torch.zeros(L.prr_padded_packet_bytes(len(p)), dtype=torch.uint8, device="cuda")
+        buf[: len(p)].copy_(torch.frombuffer(bytearray(p), dtype=torch.uint8))
+        dpk.append(buf)
+    samples = torch.empty(info0.coded_width * info0.coded_height, dtype=torch.uint16, device="cuda")
+    status = torch.zeros(4, dtype=torch.int32, device="cuda")
+    skipped = torch.zeros(info0.ntiles, dtype=torch.int32, device="cuda")
+    nscr = L.prr_decode_scratch_bytes(C.byref(info0))
+    scratch = torch.empty(nscr, dtype=torch.uint8, device="cuda")
+    ntiles = -(-W // 256) * -(-H // 256)
+    cap = ntiles * L.prr_lj92_tile_bound(256)
+    tiles = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    offsets = torch.zeros(ntiles + 1, dtype=torch.int64, device="cuda")
+    stride = info0.coded_width
+
+    def step(k, ev=None):
+        i = k % RING
+        if ev:
+            ev[0].record(s)
+        assert L.prr_decode_async(ctx, C.byref(infos[i]), dpk[i].data_ptr(), 0, samples.data_ptr(),
+                                  status.data_ptr(), skipped.data_ptr(), scratch.data_ptr(), nscr) == 0
+        if ev:
+            ev[1].record(s)
+        assert L.prr_lj92_encode(ctx, samples.data_ptr(), W, H, stride, 256, tiles.data_ptr(), cap,
+                                 offsets.data_ptr()) == 0
+        if ev:
+            ev[2].record(s)
+
+    for k in range(max(3, args.warmup)):
+        step(k)
+    torch.cuda.synchronize()
+    tile_bytes = int(offsets[-1].item())
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = L.prr_kernel_launches()
+    with Clocks(torch.cuda.current_device()) as clocks:
+        start.record(s)
+        for k in range(args.steps):
+            step(k, evs[k])
+        end.record(s)
+        torch.cuda.synchronize()
+    launches = L.prr_kernel_launches() - launches0
+    ms = start.elapsed_time(end)
+    dec_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps
+    lj_ms = sum(e[1].elapsed_time(e[2]) for e in evs) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+
+    # End to end: host packet -> DNG bytes in host memory, on DNG_THREADS
+    # host threads with a context each (one thread's container writing
+    # overlaps another's kernels).
+    clip = _lib.CDngClip()
+    clip.make, clip.fps_num, clip.fps_den, clip.orientation = b"synthetic", 30, 1, 1
+    hbufs = []
+    for p in pkts:
+        hp = torch.empty(len(p), dtype=torch.uint8, pin_memory=True)
+        hp.copy_(torch.frombuffer(bytearray(p), dtype=torch.uint8))
+        hbufs.append(hp)
+    nthreads = args.dng_threads
+    ectx, esamples, efiles = [], [], []
+    for _ in range(nthreads):
+        cx = C.c_void_p()
+        assert L.prr_ctx_create(torch.cuda.current_device(), None, C.byref(cx)) == 0
+        ectx.append(cx)
+        esamples.append(torch.empty(info0.coded_width * info0.coded_height, dtype=torch.uint16, device="cuda"))
+        # A reused pinned file buffer per thread, as a writer that saves the
+        # files would keep (twice the raw size: LJ92 never doubles it here).
+        efiles.append(torch.empty(4 * W * H, dtype=torch.uint8, pin_memory=True))
+    file_bytes = []
+
+    def e2e_worker(tid, frames, errors):
+        cx, smp, fb = ectx[tid], esamples[tid], efiles[tid]
+        res, err = _lib.CDecodeResult(), _lib.CError()
+        for k in frames:
+            hp = hbufs[k % RING]
+            rc = L.prr_decode(cx, hp.data_ptr(), hp.numel(), 0, smp.data_ptr(), smp.numel(), C.byref(res),
+                              C.byref(err))
+            nb = C.c_size_t()
+            if rc == 0:
+                rc = L.prr_dng_write_into(cx, C.byref(res.header), smp.data_ptr(), 0, 1, C.byref(clip),
+                                          fb.data_ptr(), fb.numel(), C.byref(nb))
+            if rc:
+                errors.append(rc)
+                continue
+            file_bytes.append(nb.value)
+
+    def e2e_run(nframes):
+        errors = []
+        ths = [threading.Thread(target=e2e_worker, args=(i, range(i, nframes, nthreads), errors))
+               for i in range(nthreads)]
+        t0 = time.perf_counter()
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        el = time.perf_counter() - t0
+        assert not errors, errors
+        return el
+
+    e2e_run(2 * nthreads)
+    e2e_n = max(args.steps, 4 * nthreads)
+    e2e_wall = e2e_run(e2e_n)
+    te = torch.tensor([e2e_wall], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_wall = float(te.item())
+    for cx in ectx:
+        L.prr_ctx_destroy(cx)
+    L.prr_ctx_destroy(ctx)
+    if rank == 0:
+        peak, peak_kind = peaks()
+        # The tile encoder's algorithmic bytes: the visible samples read,
+        # the streams written.
+        alg = 2 * W * H + tile_bytes
+        achieved = alg / (lj_ms / 1000.0) / 1e9
+        line = {
+            "metric": DNG_METRIC, "value": world * args.steps / (ms_max / 1000.0), "unit": "frames/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+            "data": "synthetic",
+            "config": {"workload": f"{W}x{H} BGGR v0 align4 qscale45 qmat[4,63] 0.5% corrupt tiles; decode_frame "
+                                   "(Apple) + dng::write (code values, LinearizationTable, 256-square LJ92 tiles)",
+                       "frames_in_ring": RING, "tiles_per_frame": ntiles, "tile_bytes_per_frame": tile_bytes,
+                       "dng_file_bytes": file_bytes[-1] if file_bytes else None,
+                       "l2": "35 MB of code values and about 20 MB of streams a frame; 3 distinct frames (not "
+                             "larger than L2 together: a frame's decode output is re-read by the encoder)",
+                       "parallelism": f"replicas x{world}", "decode_ms": dec_ms, "lj92_ms": lj_ms},
+            "roofline": {"bound": "hbm", "kernel": "k_lj92_encode + k_lj92_pack", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg},
+            "gpu_launches": int(launches),
+            "e2e": {"value": world * e2e_n / e2e_wall, "unit": "frames/s",
+                    "h2d_bytes_per_step": int(np.mean([len(p) for p in pkts])),
+                    "d2h_bytes_per_step": tile_bytes + 8 * (ntiles + 1) + 16,
+                    "note": f"prr_decode from a pinned host packet + prr_dng_write_into a reused pinned file "
+                            f"buffer: the DNG file's bytes in host memory, {nthreads} host threads with a context "
+                            f"each, wall clock"},
+        }
+        cl = clocks.summary()
+        if cl:
+            line["clocks"] = cl
+        if world == 1 and not args.no_cpu_baseline:
+            v, n, el, threads = dng_cpu(pkts, 15.0)
+            line["cpu_baseline"] = {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+                                    "sample": f"{n} frames: oracle decode + oracle LJ92 tiles (the crate's encoder "
+                                              f"restated), {threads} threads, {el:.1f} s; the TIFF container not "
+                                              "included"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_dng_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    pkts = make_packets(RING)
+    v, n, el, threads = dng_cpu(pkts, max(10.0, 0.2 * args.steps))
+    line = {
+        "impl": "reference", "metric": DNG_METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / n, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": f"{W}x{H} frames; decode_frame + LJ92 tiles of dng::write"},
+        "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} frames, CPU oracle decode + LJ92 tiles, {threads} threads, {el:.1f} s"},
+        "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
 # Learned develop workloads. The surrogate is trained here, on the device,
 # by the library's own kernels: 4000 random 512x512 crops of synthetic
 # 4096x2160 RGGB frames (the mosaic generator with noise sigma uniform in
@@ -1064,10 +1323,11 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="5k8", choices=["5k8", "mixed-batch", "learned", "8k-stream", "clip"],
+    ap.add_argument("--workload", default="5k8", choices=["5k8", "mixed-batch", "learned", "8k-stream", "clip", "dng"],
                     help="5k8: the headline single-frame decode+develop; mixed-batch: 64 uneven frames per step; "
                          "learned: surrogate develop of 4K frames (trains first); 8k-stream: 16 8K frames per step; "
-                         "clip: a movie file of 5.8K frames through the clip pipeline, one pass per step")
+                         "clip: a movie file of 5.8K frames through the clip pipeline, one pass per step; "
+                         "dng: 5.8K frames decoded and exported as DNG files (LJ92 tiles on the device)")
     ap.add_argument("--epochs", type=int, default=8, help="training epochs for the learned workloads")
     ap.add_argument("--save-model", default="", help="learned: save the trained surrogate (.npz)")
     ap.add_argument("--model", default=os.path.join(ROOT, "proresraw_rs_b200", "data", "surrogate.npz"),
@@ -1077,6 +1337,7 @@ def main():
     ap.add_argument("--clip-frames", type=int, default=CLIP_N, help="clip: samples in the movie")
     ap.add_argument("--clip-batch", type=int, default=CLIP_BATCH, help="clip: frames per batch")
     ap.add_argument("--clip-threads", type=int, default=CLIP_THREADS, help="clip: reader threads")
+    ap.add_argument("--dng-threads", type=int, default=4, help="dng: host threads of the end-to-end leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     args = ap.parse_args()
@@ -1084,6 +1345,8 @@ def main():
         return run_batch_reference(args) if args.impl == "reference" else run_batch(args)
     if args.workload == "clip":
         return run_clip_reference(args) if args.impl == "reference" else run_clip(args)
+    if args.workload == "dng":
+        return run_dng_reference(args) if args.impl == "reference" else run_dng(args)
     if args.workload in ("learned", "8k-stream"):
         if args.impl == "reference":
             return run_reference(args)

@@ -456,6 +456,75 @@ int prr_clip_next(prr_clip* clip, prr_clip_batch* out);
 /* The message of the last failed read or call. */
 const char* prr_clip_last_error(const prr_clip* clip);
 
+/* --- DNG export (examples/prr2dng) --------------------------------------------- */
+/* Lossless JPEG tiles of a 16-bit CFA image (DNG compression 7): the tile x
+ * tile squares of the image, row by row, each cut as dng::tile does
+ * (examples/prr2dng/dng.rs:114-125: sensels past the right or bottom edge
+ * repeat the nearest edge sensel of the same colour) and coded as
+ * lj92::encode(tile, tile, tile, 2) does (examples/prr2dng/lj92.rs:14-69),
+ * byte for byte. tile: even, 2..256 (DNG files use 256); width and height
+ * at least 2; the image's rows are `stride` samples apart. */
+uint64_t prr_lj92_tile_bound(uint32_t tile); /* worst-case bytes of one tile's stream */
+/* Asynchronous: tile i's stream at dev_out + dev_offsets[i] (device array
+ * of ntiles + 1 entries, the last the total). out_cap must hold ntiles x
+ * prr_lj92_tile_bound(tile) bytes (PRR_ERR_BUFFER otherwise). */
+int prr_lj92_encode(prr_ctx* ctx, const uint16_t* dev_image, uint32_t width, uint32_t height, uint64_t stride,
+                    uint32_t tile, uint8_t* dev_out, uint64_t out_cap, uint64_t* dev_offsets);
+/* The same into host memory (synchronous): offsets[ntiles + 1] and *total
+ * are always set; PRR_ERR_BUFFER when cap < *total. */
+int prr_lj92_encode_host(prr_ctx* ctx, const uint16_t* dev_image, uint32_t width, uint32_t height, uint64_t stride,
+                         uint32_t tile, uint8_t* out, size_t cap, uint64_t* offsets, size_t* total);
+
+/* ClipInfo (examples/prr2dng/dng.rs:46-57) and the writer's text. */
+typedef struct prr_dng_clip {
+    const char* make;      /* NULL: absent */
+    const char* model;     /* NULL: absent */
+    const char* date_time; /* "YYYY:MM:DD HH:MM:SS" (prr_dng_date_time); NULL: absent */
+    const char* software;  /* tag 305; NULL: "proresraw_rs prr2dng 0.1.0" */
+    uint32_t fps_num, fps_den; /* fps_den 0: no FrameRate */
+    uint8_t orientation;   /* EXIF 1..8 (mov Orientation); 0 counts as 1 */
+    uint8_t pad[7];
+} prr_dng_clip;
+enum prr_dng_samples { PRR_DNG_CODE_VALUES = 0, PRR_DNG_LINEAR = 1 };      /* dng::Samples */
+enum prr_dng_compression { PRR_DNG_UNCOMPRESSED = 0, PRR_DNG_LJ92 = 1 };  /* dng::Compression */
+typedef struct prr_dng_file prr_dng_file;
+
+/* dng::write (examples/prr2dng/dng.rs:77-111) of a decoded frame on the
+ * device (dev_samples: the decoder's code values over the coded size).
+ * Linear samples are linearized on the device; LJ92 tiles of 256 are
+ * encoded on the device; the TIFF container is written on the host. */
+int prr_dng_write(prr_ctx* ctx, const prr_header* header, const uint16_t* dev_samples, int samples,
+                  int compression, const prr_dng_clip* clip, prr_dng_file** out);
+/* The same into a caller's buffer (pinned memory takes the copy from the
+ * device fastest): *len is always set to the file's size; PRR_ERR_BUFFER
+ * when out is NULL or cap < *len (nothing written). */
+int prr_dng_write_into(prr_ctx* ctx, const prr_header* header, const uint16_t* dev_samples, int samples,
+                       int compression, const prr_dng_clip* clip, uint8_t* out, size_t cap, size_t* len);
+/* The container alone (host): `nchunks` chunks of `data` at offsets[0 ..
+ * nchunks] -- one strip of the visible samples (little-endian u16,
+ * uncompressed) or the frame's 256-square LJ92 tiles in order. */
+int prr_dng_assemble(const prr_header* header, const prr_dng_clip* clip, int samples, int compression,
+                     const uint8_t* data, const uint64_t* offsets, size_t nchunks, prr_dng_file** out);
+const uint8_t* prr_dng_data(const prr_dng_file* file, size_t* len);
+void prr_dng_free(prr_dng_file* file);
+
+/* DngColour (examples/prr2dng/colour.rs:58-120): the colour tags of a header. */
+typedef struct prr_dng_colour {
+    double temperature;        /* kelvin */
+    double color_matrix[9];    /* ColorMatrix1, row-major */
+    double forward_matrix[9];  /* ForwardMatrix1 */
+    double as_shot_neutral[3];
+    double baseline_exposure;  /* stops */
+    uint16_t illuminant;       /* CalibrationIlluminant1 (EXIF light source) */
+    uint8_t pad[6];
+} prr_dng_colour;
+int prr_dng_colour_of(const prr_header* header, prr_dng_colour* out);
+/* Value::srational / Value::rational (examples/prr2dng/tiff.rs:63-98). */
+int prr_dng_srational(double v, int32_t* num, int32_t* den);
+int prr_dng_rational(double v, uint32_t* num, uint32_t* den);
+/* quicktime_date_time (examples/prr2dng/dng.rs:226-246): UTC text of seconds since 1904. */
+int prr_dng_date_time(uint64_t seconds, char out[20]);
+
 /* --- diagnostics -------------------------------------------------------------- */
 /* The device inverse transforms on raw blocks (idct.rs): kind 0 Apple 8x8,
  * 1 FFmpeg 8x8, 2 Apple 4x4 (16 coefficients per block), 3 Apple 2x2 (4).

@@ -188,6 +188,34 @@ class CClipBatch(C.Structure):
         ("cuda_stream", C.c_void_p),
     ]
 
+class CDngClip(C.Structure):
+    _fields_ = [
+        ("make", C.c_char_p),
+        ("model", C.c_char_p),
+        ("date_time", C.c_char_p),
+        ("software", C.c_char_p),
+        ("fps_num", C.c_uint32),
+        ("fps_den", C.c_uint32),
+        ("orientation", C.c_uint8),
+        ("pad", C.c_uint8 * 7),
+    ]
+
+
+class CDngColour(C.Structure):
+    _fields_ = [
+        ("temperature", C.c_double),
+        ("color_matrix", C.c_double * 9),
+        ("forward_matrix", C.c_double * 9),
+        ("as_shot_neutral", C.c_double * 3),
+        ("baseline_exposure", C.c_double),
+        ("illuminant", C.c_uint16),
+        ("pad", C.c_uint8 * 6),
+    ]
+
+
+DNG_CODE_VALUES, DNG_LINEAR = 0, 1
+DNG_UNCOMPRESSED, DNG_LJ92 = 0, 1
+
 SCALE_FULL = 0
 
 _lib = None
@@ -272,6 +300,19 @@ def lib():
         "prr_clip_start": (i, [vp, C.c_uint64, C.c_uint64, i, i, i]),
         "prr_clip_next": (i, [vp, P(CClipBatch)]),
         "prr_clip_last_error": (C.c_char_p, [vp]),
+        "prr_lj92_tile_bound": (C.c_uint64, [C.c_uint32]),
+        "prr_lj92_encode": (i, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, vp, C.c_uint64, vp]),
+        "prr_lj92_encode_host": (i, [vp, vp, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, vp, sz, vp,
+                                     P(sz)]),
+        "prr_dng_write": (i, [vp, P(CHeader), vp, i, i, P(CDngClip), P(vp)]),
+        "prr_dng_write_into": (i, [vp, P(CHeader), vp, i, i, P(CDngClip), vp, sz, P(sz)]),
+        "prr_dng_assemble": (i, [P(CHeader), P(CDngClip), i, i, vp, vp, sz, P(vp)]),
+        "prr_dng_data": (P(C.c_uint8), [vp, P(sz)]),
+        "prr_dng_free": (None, [vp]),
+        "prr_dng_colour_of": (i, [P(CHeader), P(CDngColour)]),
+        "prr_dng_srational": (i, [C.c_double, P(C.c_int32), P(C.c_int32)]),
+        "prr_dng_rational": (i, [C.c_double, P(C.c_uint32), P(C.c_uint32)]),
+        "prr_dng_date_time": (i, [C.c_uint64, C.c_char_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -1,7 +1,7 @@
 """Builds the package's native libraries in-tree.
 
  - lib/libprr.so        CUDA sm_100a kernels + the C ABI of include/prr.h
-                        (and the host movie reader)
+                        (and the host movie reader and DNG container)
  - lib/libprr_synth.so  host C++ synthetic-input generator and encoder
 
 Float flags matter for bit-exactness: -fmad=false (the device code spells
@@ -30,9 +30,10 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O3",
     "-shared",
 ]
-CUDA_SOURCES = ["api.cu", "batch.cu", "clip.cu", "decode.cu", "develop.cu", "learned.cu", "noalloc.cu"]
-# Host-only parts of libprr.so (the movie reader); nvcc hands them to g++.
-HOST_SOURCES = ["mov.cpp"]
+CUDA_SOURCES = ["api.cu", "batch.cu", "clip.cu", "decode.cu", "develop.cu", "learned.cu", "lj92.cu", "noalloc.cu"]
+# Host-only parts of libprr.so (the movie reader, the DNG container); nvcc
+# hands them to g++.
+HOST_SOURCES = ["dng.cpp", "mov.cpp"]
 CXX_FLAGS = ["-O3", "-march=x86-64-v3", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-shared"]
 
 

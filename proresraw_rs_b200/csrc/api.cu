@@ -221,6 +221,14 @@ void prr_ctx_destroy(prr_ctx* c) {
     c->hskipped.release();
     c->samples.release();
     c->planes.release();
+    c->lj_words.release();
+    c->lj_lookback.release();
+    c->lj_out.release();
+    c->lj_offsets.release();
+    c->lj_flag.release();
+    c->lj_hout.release();
+    c->lj_hoffsets.release();
+    c->lin.release();
     batch_state_destroy(c->batch);
     c->batch = nullptr;
     learned_state_destroy(c->learned);

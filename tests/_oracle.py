@@ -144,6 +144,13 @@ def lib():
         L.orc_sg_loss.restype = C.c_double
         L.orc_sg_loss.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp]
         L.orc_sg_backward.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp]
+        L.orc_lj92_encode.restype = C.c_int
+        L.orc_lj92_encode.argtypes = [vp, sz, sz, sz, vp, sz, C.POINTER(C.c_size_t)]
+        L.orc_lj92_huffman.argtypes = [vp, vp, vp, C.POINTER(C.c_int), vp, vp]
+        L.orc_dng_tile.restype = C.c_int
+        L.orc_dng_tile.argtypes = [vp, sz, sz, sz, sz, sz, sz, vp]
+        L.orc_lj92_tiles.restype = C.c_int
+        L.orc_lj92_tiles.argtypes = [vp, sz, sz, sz, sz, C.c_int, vp, sz, vp]
         _lib = L
     return _lib
 
@@ -414,3 +421,47 @@ def sg_backward(in16, params, acts, dhead):
                           _p(np.ascontiguousarray(params, dtype=np.float32)), _p(np.ascontiguousarray(acts)),
                           _p(np.ascontiguousarray(dhead)), _p(dp))
     return dp
+
+
+# --- DNG export: lossless JPEG tiles (examples/prr2dng/lj92.rs, dng.rs) -------
+
+
+def lj92_encode(samples: np.ndarray, width: int, height: int, components: int = 2) -> bytes:
+    s = np.ascontiguousarray(samples, dtype=np.uint16).reshape(-1)
+    assert s.size == width * height
+    cap = C.c_size_t()
+    lib().orc_lj92_encode(_p(s), width, height, components, None, 0, C.byref(cap))
+    out = np.zeros(max(1, cap.value), dtype=np.uint8)
+    n = C.c_size_t()
+    assert lib().orc_lj92_encode(_p(s), width, height, components, _p(out), out.size, C.byref(n)) == 0
+    return out[:n.value].tobytes()
+
+
+def lj92_huffman(histogram):
+    h = np.asarray(histogram, dtype=np.uint64)
+    counts = np.zeros(16, np.uint8)
+    values = np.zeros(17, np.uint8)
+    codes = np.zeros(17, np.uint16)
+    lengths = np.zeros(17, np.uint8)
+    nv = C.c_int()
+    lib().orc_lj92_huffman(_p(h), _p(counts), _p(values), C.byref(nv), _p(codes), _p(lengths))
+    return counts, values[:nv.value], codes, lengths
+
+
+def dng_tile(values: np.ndarray, width: int, height: int, left: int, top: int, tile: int = 256,
+             stride: int = 0) -> np.ndarray:
+    v = np.ascontiguousarray(values, dtype=np.uint16).reshape(-1)
+    out = np.zeros(tile * tile, np.uint16)
+    assert lib().orc_dng_tile(_p(v), width, height, stride or width, left, top, tile, _p(out)) == 0
+    return out
+
+
+def lj92_tiles(values: np.ndarray, width: int, height: int, tile: int = 256, stride: int = 0, threads: int = 0):
+    """Every tile's stream, in order, as dng::write encodes them."""
+    v = np.ascontiguousarray(values, dtype=np.uint16).reshape(-1)
+    across, down = -(-width // tile), -(-height // tile)
+    offsets = np.zeros(across * down + 1, np.uint64)
+    cap = across * down * (2 * tile * tile * 4 + 128)
+    out = np.zeros(cap, np.uint8)
+    assert lib().orc_lj92_tiles(_p(v), width, height, stride or width, tile, threads, _p(out), cap, _p(offsets)) == 0
+    return [out[int(offsets[i]):int(offsets[i + 1])].tobytes() for i in range(across * down)]
