@@ -10,11 +10,13 @@ planes, more than the 126 MB L2, so no step reads a previous step's data
 from L2.
 
  value  frames/s with the packets resident in HBM, CUDA-event timed on the
-        stream the kernels run on, max over ranks.
+        streams the kernels run on (frame k+1 decodes on a higher-priority
+        stream while frame k develops), max over ranks.
  e2e    frames/s through the host-buffer C-ABI call prr_decode_develop_host:
         pinned host packet in, pinned host planes out, copies included.
  roofline  the develop kernel's algorithmic bytes (2 B read + 12 B written
-        per visible sensel) over its event-timed duration.
+        per visible sensel) over its event-timed duration in the timed
+        region, where it shares the SMs with the next frame's decode.
  cpu_baseline  the CPU oracle (the crate's algorithm restated in C++,
         threaded like rayon) on a bounded sample of the same frames.
 
@@ -259,15 +261,26 @@ def run(args):
     info0 = infos[0]
     n = W * H
     torch.cuda.synchronize()
-    # One stream: decode then develop, frame after frame. (Decoding frame k+1
-    # on a second stream while frame k develops was measured slower: the
-    # latency-bound entropy warps lose issue slots to the develop kernel.)
-    s_dec = torch.cuda.Stream()
-    s_dev = s_dec
     dev_index = torch.cuda.current_device()
+    if args.overlap:
+        # Two streams: frame k+1 decodes while frame k develops. The decode
+        # stream has the higher priority, so the block scheduler gives it
+        # each slot a develop CTA frees; --develop-ctas can cap the develop
+        # (measured slower: 3 per SM 1860 frames/s, 2 per SM 1463, against
+        # 2072 uncapped).
+        s_dec = torch.cuda.Stream(priority=-1)
+        s_dev = torch.cuda.Stream(priority=0)
+    else:
+        # One stream: decode then develop, frame after frame.
+        s_dec = torch.cuda.Stream()
+        s_dev = s_dec
     ctx_dec = C.c_void_p()
     assert L.prr_ctx_create(dev_index, C.c_void_p(s_dec.cuda_stream), C.byref(ctx_dec)) == 0
     ctx_dev = ctx_dec
+    if args.overlap:
+        ctx_dev = C.c_void_p()
+        assert L.prr_ctx_create(dev_index, C.c_void_p(s_dev.cuda_stream), C.byref(ctx_dev)) == 0
+        assert L.prr_develop_set_occupancy(ctx_dev, args.develop_ctas) == 0
 
     # Device-resident packets (padded), scratch, outputs.
     dpk = []
@@ -345,6 +358,8 @@ def run(args):
     dec_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps
     dev_ms = sum(e[2].elapsed_time(e[3]) for e in evs) / args.steps
     L.prr_ctx_destroy(ctx_dec)
+    if ctx_dev.value != ctx_dec.value:
+        L.prr_ctx_destroy(ctx_dev)
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -370,7 +385,10 @@ def run(args):
                        "frames_in_ring": RING, "packet_bytes": [len(p) for p in pkts],
                        "l2": "inputs+outputs > L2 (210 MB planes written per step)",
                        "parallelism": f"replicas x{world}",
-                       "decode_ms": dec_ms, "develop_ms": dev_ms},
+                       "decode_ms": dec_ms, "develop_ms": dev_ms,
+                       "streams": ("decode of frame k+1 on a higher-priority stream beside develop of frame k"
+                                   + (f" (at most {args.develop_ctas} develop CTAs per SM)" if args.develop_ctas
+                                      else "")) if args.overlap else "one stream"},
             "roofline": {"bound": "hbm", "kernel": "k_develop", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs",
@@ -1338,6 +1356,10 @@ def main():
     ap.add_argument("--clip-batch", type=int, default=CLIP_BATCH, help="clip: frames per batch")
     ap.add_argument("--clip-threads", type=int, default=CLIP_THREADS, help="clip: reader threads")
     ap.add_argument("--dng-threads", type=int, default=4, help="dng: host threads of the end-to-end leg")
+    ap.add_argument("--overlap", action=argparse.BooleanOptionalAction, default=True,
+                    help="5k8: decode frame k+1 on a second, higher-priority stream while frame k develops")
+    ap.add_argument("--develop-ctas", type=int, default=0,
+                    help="5k8 --overlap: cap the develop at this many CTAs per SM (0: as many as fit)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     args = ap.parse_args()

@@ -352,6 +352,11 @@ int prr_sg_trainer_step(prr_sg_trainer* t, const uint32_t* crops, float lr, floa
 int prr_sg_gradients(prr_ctx* ctx, const float* in16, const float* base3, const float* target3, uint32_t hq,
                      uint32_t wq, const float* params, float* head_out, float* dparams, double* loss);
 
+/* Cap prr_develop at `ctas_per_sm` CTAs per SM (0: as many as fit, the
+ * default), so that kernels of another stream -- the next frame's decode --
+ * find room on every SM while this context's develop runs. */
+int prr_develop_set_occupancy(prr_ctx* ctx, uint32_t ctas_per_sm);
+
 /* --- host-buffer conveniences (synchronous) ----------------------------------- */
 /* decode_frame_with + develop_planar_into / develop_into with host input and
  * host outputs: uploads the packet, decodes and develops on the device and

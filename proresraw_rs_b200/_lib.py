@@ -263,6 +263,7 @@ def lib():
         "prr_params_with_white_balance": (i, [P(CHeader), C.c_uint32, C.c_float, C.c_float, P(CParams)]),
         "prr_output_matrix": (i, [P(CHeader), i, vp]),
         "prr_develop": (i, [vp, P(CHeader), P(CParams), i, vp, i, vp, vp, vp, sz]),
+        "prr_develop_set_occupancy": (i, [vp, C.c_uint32]),
         "prr_decode_develop_host": (i, [vp, vp, sz, i, P(CParams), i, i, vp, vp, vp, sz, P(CDecodeResult),
                                         P(CError)]),
         "prr_transform_blocks": (i, [vp, i, vp, vp, vp, sz]),

@@ -544,6 +544,7 @@ int develop_launch(prr_ctx* c, const prr_header* h, const prr_params* params, in
     DevelopDesc d{};
     PRR_TRY(build_develop_desc(h, params, stage, dev_samples, layout, r, g, b, out_len, &d));
     PRR_TRY(c->use_device());
+    d.ctas_per_sm = c->develop_ctas;
     return c->cuda(launch_develop(d, c->stream));
 }
 
@@ -666,3 +667,9 @@ int prr_decode_components(prr_ctx* c, const uint8_t* packet, const uint32_t* off
 }
 
 }  // extern "C"
+
+extern "C" int prr_develop_set_occupancy(prr_ctx* c, uint32_t ctas_per_sm) {
+    if (!c || ctas_per_sm > 16) return PRR_ERR_INVALID;
+    c->develop_ctas = ctas_per_sm;
+    return PRR_OK;
+}

@@ -82,6 +82,7 @@ struct prr_ctx {
     HostBuf<uint8_t> lj_hout;
     HostBuf<uint64_t> lj_hoffsets;
     DevBuf<uint16_t> lin;
+    uint32_t develop_ctas = 0;  // prr_develop_set_occupancy
     prr::BatchState* batch = nullptr;
     prr::LearnedState* learned = nullptr;
     std::string last_error;

@@ -19,6 +19,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -188,6 +190,11 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
         }
     }
     __syncthreads();
+    // mirror() changes a neighbour only for sites within 2 sensels of a
+    // picture edge; the green-pass sites of a tile lie within [x0 - 1,
+    // x0 + TW] x [y0 - 1, y0 + TH], so tiles clear of the edges skip it
+    // (a branch uniform over the block).
+    const bool near_edge = x0 < 3 || x0 + TW + 3 > w || y0 < 3 || y0 + TH + 3 > h;
     // 2. Green pass on the region: red/blue sites first (the heavy ones),
     //    17 per region row, then green sites.
     for (int k = tid; k < GH * (GW / 2) * 2; k += kDevThreads) {
@@ -212,8 +219,10 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
                            fminf(S.nrm[ty][tx - 2], clip), fminf(S.nrm[ty][tx + 2], clip)};
             float vv[4] = {fminf(S.nrm[ty - 1][tx], 1.0f), fminf(S.nrm[ty + 1][tx], 1.0f),
                            fminf(S.nrm[ty - 2][tx], clip), fminf(S.nrm[ty + 2][tx], clip)};
-            mirror(hh, x, w, c);
-            mirror(vv, y, h, c);
+            if (near_edge) {
+                mirror(hh, x, w, c);
+                mirror(vv, y, h, c);
+            }
             float var_h[4], var_v[4], sd_h[4], sd_v[4];
             float sdc;
             if (PRE) {
@@ -229,10 +238,12 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
                 sd_h[2] = S.gsd[ty][tx - 2]; sd_h[3] = S.gsd[ty][tx + 2];
                 sd_v[0] = S.gsd[ty - 1][tx]; sd_v[1] = S.gsd[ty + 1][tx];
                 sd_v[2] = S.gsd[ty - 2][tx]; sd_v[3] = S.gsd[ty + 2][tx];
-                mirror(var_h, x, w, vc);
-                mirror(var_v, y, h, vc);
-                mirror(sd_h, x, w, sdc);
-                mirror(sd_v, y, h, sdc);
+                if (near_edge) {
+                    mirror(var_h, x, w, vc);
+                    mirror(var_v, y, h, vc);
+                    mirror(sd_h, x, w, sdc);
+                    mirror(sd_v, y, h, sdc);
+                }
             } else {
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
@@ -416,13 +427,61 @@ cudaError_t launch_linearize(const uint16_t* codes, uint32_t stride, int w, int 
     return cudaGetLastError();
 }
 
+namespace {
+
+// Dynamic shared memory that caps k_develop<PRE> at `ctas` CTAs per SM
+// (0: none), found with the occupancy calculator and kept per cap.
+template <bool PRE>
+cudaError_t develop_reserve(uint32_t ctas, size_t* bytes) {
+    *bytes = 0;
+    if (ctas == 0) return cudaSuccess;
+    static size_t cache[2][17] = {};
+    static bool known[2][17] = {};
+    if (ctas <= 16 && known[PRE][ctas]) {
+        *bytes = cache[PRE][ctas];
+        return cudaSuccess;
+    }
+    int dev = 0, per_sm = 0, per_block = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    // A block's static plus dynamic shared memory above 48 KB needs the
+    // opt-in limit.
+    e = cudaFuncSetAttribute(k_develop<PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(std::min<size_t>(size_t(per_block) - sizeof(DevShared), size_t(per_sm))));
+    if (e != cudaSuccess) return e;
+    const size_t step = 1024;
+    size_t pad = 0;
+    for (;;) {
+        int n = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_develop<PRE>, kDevThreads, pad);
+        if (e != cudaSuccess) return e;
+        if (n <= int(ctas) || pad + sizeof(DevShared) + step > size_t(per_block)) break;
+        pad += step;
+    }
+    if (ctas <= 16) {
+        cache[PRE][ctas] = pad;
+        known[PRE][ctas] = true;
+    }
+    *bytes = pad;
+    return cudaSuccess;
+}
+
+}  // namespace
+
 cudaError_t launch_develop(const DevelopDesc& d, cudaStream_t s) {
     if (d.w <= 0 || d.h <= 0) return cudaSuccess;
     dim3 grid((d.w + TW - 1) / TW, (d.h + TH - 1) / TH);
-    if (d.w >= 4 && d.h >= 4)
-        k_develop<true><<<grid, kDevThreads, 0, s>>>(d);
-    else
-        k_develop<false><<<grid, kDevThreads, 0, s>>>(d);
+    size_t pad = 0;
+    cudaError_t e;
+    if (d.w >= 4 && d.h >= 4) {
+        if ((e = develop_reserve<true>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
+        k_develop<true><<<grid, kDevThreads, pad, s>>>(d);
+    } else {
+        if ((e = develop_reserve<false>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
+        k_develop<false><<<grid, kDevThreads, pad, s>>>(d);
+    }
     count_launch();
     return cudaGetLastError();
 }

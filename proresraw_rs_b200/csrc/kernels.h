@@ -135,6 +135,9 @@ struct DevelopDesc {
     // Non-null: develop only the 32x32 tiles whose byte is nonzero (row-major
     // over the tile grid).
     const uint8_t* tile_mask;
+    // Nonzero: at most this many CTAs per SM (shared memory reserved per
+    // CTA), leaving room for kernels of other streams.
+    uint32_t ctas_per_sm;
 };
 
 constexpr int kDevelopTile = 32;
