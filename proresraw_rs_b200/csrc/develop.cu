@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "device_common.cuh"
 #include "kernels.h"
@@ -130,6 +131,40 @@ constexpr int NW = TW + 6, NH = TH + 6;   // normalized values, 3-sensel halo
 constexpr int GW = TW + 2, GH = TH + 2;   // green-pass region, 1-sensel halo
 constexpr int kDevThreads = 256;          // one thread per 2x2 quad of the tile
 
+// The tile's code values with the halo, as one TMA box: 38 rows of 48
+// sensels from x0 - 8 (the box's first column must sit on a 16-byte
+// boundary), of which columns 5 .. 42 are the 38 the tile reads.
+constexpr int kBoxW = 48, kBoxX = 5;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Phase 0 of the tile's barrier, for at most about `limit_ns`.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint64_t limit_ns) {
+    if (bar_try_wait(bar, 0)) return true;
+    uint64_t t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (uint32_t i = 0; i < (1u << 24); i++) {
+        if (bar_try_wait(bar, 0)) return true;
+        __nanosleep(64);
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > limit_ns) return false;
+    }
+    return false;
+}
+
 struct DevShared {
     float nrm[NH][NW];
     // Green-pass noise terms of every normalized value once clipped at its
@@ -156,18 +191,39 @@ struct DevShared {
 // assumes (green at distance 1, the centre's colour at distance 2). Frames 2
 // sensels wide or tall keep the direct evaluation.
 template <bool PRE>
-__global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
+__global__ void __launch_bounds__(kDevThreads) k_develop(const __grid_constant__ CUtensorMap codes_map,
+                                                         DevelopDesc d) {
     __shared__ DevShared S;
+    __shared__ __align__(128) uint16_t box[NH][kBoxW];
+    __shared__ __align__(8) uint64_t box_bar;
     // Only the tiles a mask selects (the learned develop's fallback tiles).
     if (d.tile_mask && !d.tile_mask[blockIdx.y * gridDim.x + blockIdx.x]) return;
     const int tid = threadIdx.x;
     const int w = d.w, h = d.h;
     const int x0 = blockIdx.x * TW, y0 = blockIdx.y * TH;
+    // Tiles whose halo lies inside the picture (no clamping) load their code
+    // values with one TMA box; the others clamp each coordinate.
+    const bool tma = d.use_tma && x0 >= 3 && x0 + TW + 3 <= w && y0 >= 3 && y0 + TH + 3 <= h;
+    const uint32_t bar = smem_addr(&box_bar);
     if (tid < 8) {
         S.c0[tid] = d.curve_c0[tid];
         S.cd[tid] = d.curve_delta[tid];
     }
+    if (tma && tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(uint32_t(sizeof(box))), "r"(bar)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
+                "r"(smem_addr(&box[0][0])),
+            "l"(reinterpret_cast<uint64_t>(&codes_map)), "r"(bar), "r"(x0 - 8), "r"(y0 - 3)
+            : "memory");
+    }
     __syncthreads();
+    // A box that has not landed within a second (it always should) leaves the
+    // tile to the clamped loads, which give the same values.
+    const bool staged = tma && bar_wait(bar, 1000000000ull);
     const Noise nz{d.noise[0], d.noise[1], d.noise[2]};
     const int red_row = d.cfa >> 1, red_col = d.cfa & 1;
     // 1. Normalized values, coordinates clamped to the picture as the green
@@ -176,7 +232,7 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
         const int ty = i / NW, tx = i - ty * NW;
         const int y = min(max(y0 - 3 + ty, 0), h - 1);
         const int x = min(max(x0 - 3 + tx, 0), w - 1);
-        const uint32_t code = __ldg(d.codes + size_t(y) * d.stride + x);
+        const uint32_t code = staged ? uint32_t(box[ty][tx + kBoxX]) : uint32_t(__ldg(d.codes + size_t(y) * d.stride + x));
         const int32_t lin = int32_t(curve_apply(S.c0, S.cd, code));
         const float v = mul(d.one_over_range, __int2float_rn(lin - d.black));
         S.nrm[ty][tx] = v;
@@ -190,6 +246,7 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(DevelopDesc d) {
         }
     }
     __syncthreads();
+    if (tma && !staged && tid == 0) bar_wait(bar, 1000000000ull);  // a late box lands before the CTA ends
     // mirror() changes a neighbour only for sites within 2 sensels of a
     // picture edge; the green-pass sites of a tile lie within [x0 - 1,
     // x0 + TW] x [y0 - 1, y0 + TH], so tiles clear of the edges skip it
@@ -470,17 +527,29 @@ cudaError_t develop_reserve(uint32_t ctas, size_t* bytes) {
 
 }  // namespace
 
-cudaError_t launch_develop(const DevelopDesc& d, cudaStream_t s) {
-    if (d.w <= 0 || d.h <= 0) return cudaSuccess;
+cudaError_t launch_develop(const DevelopDesc& desc, cudaStream_t s) {
+    if (desc.w <= 0 || desc.h <= 0) return cudaSuccess;
+    DevelopDesc d = desc;
     dim3 grid((d.w + TW - 1) / TW, (d.h + TH - 1) / TH);
+    // The code values as a 2-D tensor (rows of the coded width, the
+    // picture's height) for the TMA tile loads; a buffer that is not 16-byte
+    // aligned, or a map the driver refuses, leaves every tile to the
+    // clamped loads.
+    alignas(64) CUtensorMap map;
+    std::memset(&map, 0, sizeof(map));
+    d.use_tma = 0;
+    if ((reinterpret_cast<uintptr_t>(d.codes) & 15) == 0 && (d.stride * 2) % 16 == 0 && d.w >= TW + 6 &&
+        d.h >= TH + 6)
+        d.use_tma = encode_u16_map_2d(&map, d.codes, d.stride, uint64_t(d.h), uint64_t(d.stride) * 2, kBoxW, NH) ==
+                    cudaSuccess;
     size_t pad = 0;
     cudaError_t e;
     if (d.w >= 4 && d.h >= 4) {
         if ((e = develop_reserve<true>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
-        k_develop<true><<<grid, kDevThreads, pad, s>>>(d);
+        k_develop<true><<<grid, kDevThreads, pad, s>>>(map, d);
     } else {
         if ((e = develop_reserve<false>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
-        k_develop<false><<<grid, kDevThreads, pad, s>>>(d);
+        k_develop<false><<<grid, kDevThreads, pad, s>>>(map, d);
     }
     count_launch();
     return cudaGetLastError();

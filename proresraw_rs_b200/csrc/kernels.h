@@ -1,6 +1,7 @@
 // kernels.h -- host-side launchers of the library's CUDA kernels.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -138,6 +139,8 @@ struct DevelopDesc {
     // Nonzero: at most this many CTAs per SM (shared memory reserved per
     // CTA), leaving room for kernels of other streams.
     uint32_t ctas_per_sm;
+    // Set by launch_develop: interior tiles load their code values by TMA.
+    uint32_t use_tma;
 };
 
 constexpr int kDevelopTile = 32;
@@ -152,5 +155,9 @@ cudaError_t launch_linearize(const uint16_t* codes, uint32_t stride, int w, int 
                              const uint32_t* c0, const uint32_t* delta, uint16_t* out,
                              cudaStream_t s);
 cudaError_t launch_develop(const DevelopDesc& d, cudaStream_t s);
+// learned.cu: a 2-D tensor map of 16-bit elements (cuTensorMapEncodeTiled
+// through the runtime's driver entry point).
+cudaError_t encode_u16_map_2d(CUtensorMap* map, const void* base, uint64_t width, uint64_t height,
+                              uint64_t row_bytes, uint32_t box_w, uint32_t box_h);
 
 }  // namespace prr

@@ -1453,3 +1453,29 @@ int prr_sg_gradients(prr_ctx* c, const float* in16, const float* base3, const fl
 }
 
 }  // extern "C"
+
+namespace prr {
+
+// A 2-D tensor map of 16-bit elements: `width` x `height`, rows `row_bytes`
+// apart (a multiple of 16), boxes of box_w x box_h, no swizzle.
+cudaError_t encode_u16_map_2d(CUtensorMap* map, const void* base, uint64_t width, uint64_t height,
+                              uint64_t row_bytes, uint32_t box_w, uint32_t box_h) {
+    static sg::EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return e != cudaSuccess ? e : cudaErrorUnknown;
+        fn = reinterpret_cast<sg::EncodeTiledFn>(p);
+    }
+    const cuuint64_t dims[2] = {width, height};
+    const cuuint64_t strides[1] = {row_bytes};
+    const cuuint32_t box[2] = {box_w, box_h};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+}  // namespace prr
