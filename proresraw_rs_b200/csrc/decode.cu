@@ -800,15 +800,56 @@ __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off,
 // on average. Larger spans are read from global memory instead.
 constexpr uint32_t kStageBytes = 32 * 1024;
 
+// One component stream of a chunk: where its bytes and its list are.
+struct StreamJob {
+    bool valid;
+    uint32_t g, s, trow, x, log2, soff, slen;
+};
+
+// Stream g of the frame (tile g / 4, component g % 4): Tile::parse
+// (src/tile.rs:126-153) of its tile's header and the stream's span; not
+// valid when there is nothing to decode (past the last tile, a second green
+// a reduced decode does not average, an invalid tile -- left to the
+// transform kernel, which records it).
+template <uint32_t LC>
+__device__ __forceinline__ StreamJob stream_job(const FrameDesc& d, int greens, const uint32_t* __restrict__ tile_off,
+                                                uint32_t g) {
+    StreamJob j{};
+    j.g = g;
+    if (g >= 4 * d.ntiles) return j;
+    const uint32_t tile = g >> 2, s = g & 3;
+    if (LC != 6 && s == 1 && !greens) return j;  // a reduced decode reads the second green only to average
+    j.s = s;
+    j.trow = tile / d.tiles_per_row;
+    const uint32_t col = tile - j.trow * d.tiles_per_row;
+    tile_geom(col, d.columns, d.alignment, j.x, j.log2);
+    const uint32_t off = tile_off[tile], end = tile_off[tile + 1];
+    if (!(off <= end && end <= d.len) || end - off < 8) return j;
+    const uint32_t size = end - off;
+    const uint32_t header_len = byte_at(d.words, off) >> 3;
+    const uint32_t qscale = byte_at(d.words, off + 1);
+    const uint32_t s0 = be16_at(d.words, off + 2), s1 = be16_at(d.words, off + 4), s2 = be16_at(d.words, off + 6);
+    const uint32_t used = header_len + s0 + s1 + s2;
+    if (!(header_len >= 8 && qscale != 0 && s0 != 0 && s1 != 0 && s2 != 0 && used < size)) return j;
+    j.soff = off + header_len + (s > 0 ? s0 : 0) + (s > 1 ? s1 : 0) + (s > 2 ? s2 : 0);
+    j.slen = s == 0 ? s0 : s == 1 ? s1 : s == 2 ? s2 : size - used;
+    j.valid = true;
+    return j;
+}
+
 // Entropy-decode the streams of tiles [chunk * blockDim.x / 4, ...) of a
 // frame, one stream per thread. `stage` holds stage_bytes + 16 bytes of
 // shared memory; the chunk's packet span is copied there when it fits.
-// Ends with the CTA's threads at different points (no barrier).
-template <uint32_t LC>
+// With SORT, the threads take the chunk's streams in order of their byte
+// length, so that the 32 lanes of a warp decode streams of about the same
+// number of symbols and stay busy together (a warp loops until its longest
+// stream ends). Ends with the CTA's threads at different points (no
+// barrier).
+template <uint32_t LC, bool SORT>
 __device__ __forceinline__ void entropy_chunk(const EntropyTables& T, uint32_t* stage, uint32_t stage_bytes,
                                               const FrameDesc& d, int greens,
                                               const uint32_t* __restrict__ tile_off, prr_dev_status* st,
-                                              uint32_t chunk) {
+                                              uint32_t chunk, uint32_t* keys = nullptr) {
     // The chunk's tiles [t0, t1) occupy bytes [tile_off[t0], tile_off[t1]).
     const uint32_t t0 = chunk * (blockDim.x / 4);
     const uint32_t t1 = min(t0 + blockDim.x / 4, d.ntiles);
@@ -824,31 +865,40 @@ __device__ __forceinline__ void entropy_chunk(const EntropyTables& T, uint32_t* 
             dst[i] = make_uint4(bswap32(v.x), bswap32(v.y), bswap32(v.z), bswap32(v.w));
         }
     }
-    __syncthreads();
-    const uint32_t g = chunk * blockDim.x + threadIdx.x;
-    if (g >= 4 * d.ntiles) return;
-    const uint32_t tile = g >> 2, s = g & 3;
-    if (LC != 6 && s == 1 && !greens) return;  // a reduced decode reads the second green only to average
-    const uint32_t trow = tile / d.tiles_per_row, j = tile - trow * d.tiles_per_row;
-    uint32_t x, log2;
-    tile_geom(j, d.columns, d.alignment, x, log2);
-    const uint32_t off = tile_off[tile], end = tile_off[tile + 1];
-    if (!(off <= end && end <= d.len) || end - off < 8) return;
-    const uint32_t size = end - off;
-    const uint32_t header_len = byte_at(d.words, off) >> 3;
-    const uint32_t qscale = byte_at(d.words, off + 1);
-    const uint32_t s0 = be16_at(d.words, off + 2), s1 = be16_at(d.words, off + 4), s2 = be16_at(d.words, off + 6);
-    const uint32_t used = header_len + s0 + s1 + s2;
-    if (!(header_len >= 8 && qscale != 0 && s0 != 0 && s1 != 0 && s2 != 0 && used < size)) return;
-    const uint32_t soff = off + header_len + (s > 0 ? s0 : 0) + (s > 1 ? s1 : 0) + (s > 2 ? s2 : 0);
-    const uint32_t slen = s == 0 ? s0 : s == 1 ? s1 : s == 2 ? s2 : size - used;
-    uint32_t* list = d.pairs + stream_list_base(d, trow, x, log2, s, LC);
+    StreamJob job = stream_job<LC>(d, greens, tile_off, chunk * blockDim.x + threadIdx.x);
+    if (SORT) {
+        // Bitonic sort of (length << 9 | thread) over the block (a power of
+        // two, at most 512 threads) in `keys` (shared, a word per thread);
+        // thread i then takes the stream of the i-th key.
+        keys[threadIdx.x] = (job.valid ? (min(job.slen, 0x7FFFFFu) << 9) : 0u) | threadIdx.x;
+        __syncthreads();
+        const uint32_t n = blockDim.x, i = threadIdx.x;
+        for (uint32_t k = 2; k <= n; k <<= 1) {
+            for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+                const uint32_t p = i ^ jj;
+                if (p > i) {
+                    const uint32_t a = keys[i], b = keys[p];
+                    if ((a > b) == ((i & k) == 0)) {
+                        keys[i] = b;
+                        keys[p] = a;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        const uint32_t src = keys[i] & 511;
+        if (src != i) job = stream_job<LC>(d, greens, tile_off, chunk * blockDim.x + src);
+    } else {
+        __syncthreads();
+    }
+    if (!job.valid) return;
+    uint32_t* list = d.pairs + stream_list_base(d, job.trow, job.x, job.log2, job.s, LC);
     bool revisited = false, ok = true;
     const uint32_t cnt =
-        staged ? entropy_events<LC>(StagedWords{stage, base >> 2}, soff, slen, log2, T, list, revisited, ok)
-               : entropy_events<LC>(PacketWords{d.words}, soff, slen, log2, T, list, revisited, ok);
+        staged ? entropy_events<LC>(StagedWords{stage, base >> 2}, job.soff, job.slen, job.log2, T, list, revisited, ok)
+               : entropy_events<LC>(PacketWords{d.words}, job.soff, job.slen, job.log2, T, list, revisited, ok);
     if (!ok) atomicOr(&st->error, 1u);
-    d.counts[g] = revisited ? 0x80000000u : cnt;
+    d.counts[job.g] = revisited ? 0x80000000u : cnt;
 }
 
 template <uint32_t LC>
@@ -860,7 +910,7 @@ __global__ void __launch_bounds__(128) k_entropy(FrameDesc d, int greens, const 
     load_tables(&CT);
     __syncthreads();
     build_entropy_tables(T, CT);
-    entropy_chunk<LC>(T, stage, kStageBytes, d, greens, tile_off, st, blockIdx.x);
+    entropy_chunk<LC, false>(T, stage, kStageBytes, d, greens, tile_off, st, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -999,8 +1049,8 @@ __device__ __forceinline__ uint32_t batch_frame_of(const BatchDesc& b, uint32_t 
 template <uint32_t LC>
 __device__ __noinline__ void batch_entropy(const EntropyTables& T, uint32_t* stage, uint32_t stage_bytes,
                                            const FrameDesc& d, int greens, const uint32_t* tile_off,
-                                           prr_dev_status* st, uint32_t chunk) {
-    entropy_chunk<LC>(T, stage, stage_bytes, d, greens, tile_off, st, chunk);
+                                           prr_dev_status* st, uint32_t chunk, uint32_t* keys) {
+    entropy_chunk<LC, true>(T, stage, stage_bytes, d, greens, tile_off, st, chunk, keys);
 }
 template <int IDCT>
 __device__ __noinline__ void batch_full(SegShared& S, const FrameDesc& d, uint32_t seg, uint32_t trow,
@@ -1026,6 +1076,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
     __shared__ EntropyTables T;
     __shared__ FrameDesc fd;
     __shared__ uint32_t s_item, s_frame, s_epoch, s_ok;
+    __shared__ uint32_t keys[kBatchThreads];  // the entropy chunks' stream order
     const uint32_t tid = threadIdx.x;
     load_tables(&S.T);
     if (tid == 0) s_epoch = b.q->epoch;
@@ -1054,11 +1105,11 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
             __syncthreads();
             const uint32_t chunk = item - F.ent_begin;
             if (lc == 6)
-                batch_entropy<6>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk);
+                batch_entropy<6>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk, keys);
             else if (lc == 4)
-                batch_entropy<4>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk);
+                batch_entropy<4>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk, keys);
             else
-                batch_entropy<2>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk);
+                batch_entropy<2>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk, keys);
             __syncthreads();
             if (tid == 0) {
                 __threadfence();
