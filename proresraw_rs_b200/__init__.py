@@ -213,12 +213,16 @@ class FrameHeader:
 
 
 def _pkt(packet) -> Tuple[object, int]:
-    """(pointer, length) of a bytes-like or numpy packet in host memory."""
+    """(buffer, length) of a bytes-like or numpy packet in host memory: a
+    uint8 view of the caller's bytes, not a copy (the library only reads
+    them)."""
     if isinstance(packet, np.ndarray):
-        a = np.ascontiguousarray(packet, dtype=np.uint8)
-        return a, a.size
-    b = bytes(packet)
-    return C.create_string_buffer(b, max(1, len(b))), len(b)
+        a = np.ascontiguousarray(packet, dtype=np.uint8).reshape(-1)
+    else:
+        a = np.frombuffer(packet, dtype=np.uint8)
+    if a.size == 0:
+        return np.zeros(1, dtype=np.uint8), 0
+    return a, a.size
 
 
 def _ptr(obj) -> int:

@@ -231,6 +231,34 @@ int check_config(const prr_batch_config& c) {
     return PRR_OK;
 }
 
+// The jobs' packets into the pinned staging buffer at their planned
+// offsets. A large batch is copied by several host threads, each taking
+// an equal share of the bytes (a copy from pageable memory runs at a few
+// GB/s a thread).
+void stage_packets(uint8_t* dst, const prr_job* jobs, const std::vector<FramePlan>& plan, size_t total) {
+    const size_t kPerThread = size_t(16) << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nthreads = unsigned(std::min<size_t>({size_t(hw), size_t(16), total / kPerThread + 1}));
+    auto copy_range = [&](size_t lo, size_t hi) {
+        // Bytes [lo, hi) of the staging buffer: the parts of the frames there.
+        for (const FramePlan& f : plan) {
+            const size_t a = f.pkt_off, b = f.pkt_off + size_t(jobs[f.job].len);
+            const size_t x = std::max(a, lo), y = std::min(b, hi);
+            if (x < y) std::memcpy(dst + x, jobs[f.job].packet + (x - a), y - x);
+        }
+    };
+    if (nthreads <= 1) {
+        copy_range(0, total);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t share = (total + nthreads - 1) / nthreads;
+    for (unsigned k = 1; k < nthreads; k++)
+        pool.emplace_back(copy_range, std::min(total, k * share), std::min(total, (k + 1) * share));
+    copy_range(0, std::min(total, share));
+    for (auto& th : pool) th.join();
+}
+
 // Enqueue the batch's kernels and the status download (directly, or as the
 // bucket's graph).
 int enqueue_kernels(prr_ctx* c, BatchState* B, Bucket& bk, const prr_batch_config& cfg, const BatchDesc& desc,
@@ -342,7 +370,6 @@ int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force, c
     for (size_t i = 0; i < nf; i++) {
         const FramePlan& f = B->plan[i];
         const prr_job& j = jobs[f.job];
-        if (!staged) std::memcpy(B->hpackets.p + f.pkt_off, j.packet, size_t(j.len));
         BatchFrame& F = hf[i];
         std::memset(&F, 0, sizeof(F));
         F.d = make_frame_desc(f.info, B->packets.p + f.pkt_off);
@@ -363,6 +390,7 @@ int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force, c
         ent += (ntiles + kBatchTilesPerChunk - 1) / kBatchTilesPerChunk;
         seg += f.info.tile_rows * F.d.segs_per_row;
     }
+    if (!staged) stage_packets(B->hpackets.p, jobs, B->plan, t.packet_bytes);
     PRR_TRY(c->cuda(cudaMemcpyAsync(B->meta.p, B->hmeta.p, sizeof(BatchHeader) + nf * sizeof(BatchFrame),
                                     cudaMemcpyHostToDevice, c->stream)));
     PRR_TRY(c->cuda(cudaMemcpyAsync(B->packets.p, staged ? staged : B->hpackets.p, t.packet_bytes,
