@@ -379,3 +379,46 @@ def test_footage_clips():
     path = os.path.join(root, "iphone17-prores_raw/01_A001_09211049_C068.mov")
     if os.path.isfile(path):
         assert read(path).orientation == O.ROTATE_180
+
+
+def test_corrupted_movies_fail_cleanly(tmp_path):
+    # Random byte changes, truncations and size-field rewrites of valid
+    # movies (with metadata, edit lists, both offset widths): every read
+    # either succeeds or raises the crate's error, never crashes.
+    import random
+
+    rng = random.Random(12)
+    bases = [
+        M.movie_bytes([Spec(edits=[(40, -1), (40, 40)], co64=True)], creation=5,
+                      meta=M.meta_atom([("a", "b"), ("c", b"\x00\x01")])),
+        M.movie_bytes([Spec(size_table="stz2", stz2_bits=4), Spec(handler=b"soun")]),
+        M.movie_bytes([Spec(tkhd_version=1, matrix=(0, ONE, -ONE, 0))], meta=M.meta_atom([("k", "v")], iso=True)),
+    ]
+    path = tmp_path / "fuzz.mov"
+    outcomes = {"ok": 0, "error": 0}
+    for trial in range(600):
+        data = bytearray(rng.choice(bases))
+        kind = rng.randrange(4)
+        if kind == 0:  # random bytes
+            for _ in range(rng.randrange(1, 8)):
+                data[rng.randrange(len(data))] = rng.randrange(256)
+        elif kind == 1:  # truncation
+            del data[rng.randrange(1, len(data)):]
+        elif kind == 2:  # a 32-bit field set to an extreme
+            at = rng.randrange(0, len(data) - 4)
+            data[at:at + 4] = struct.pack(">I", rng.choice([0, 1, 2, 7, 8, 0x7FFFFFFF, 0xFFFFFFFF, len(data)]))
+        else:  # an atom's size field grown or shrunk
+            at = data.find(rng.choice([b"trak", b"stbl", b"stsz", b"stsc", b"meta", b"keys", b"elst", b"tkhd"]))
+            if at >= 4:
+                size = struct.unpack(">I", data[at - 4:at])[0]
+                data[at - 4:at] = struct.pack(">I", max(0, size + rng.choice([-9, -1, 1, 9, 1000])) & 0xFFFFFFFF)
+        path.write_bytes(bytes(data))
+        try:
+            with read(path) as t:
+                for s in t.samples[:3]:
+                    buf = bytearray(s.size)
+                    mov.read_at(t, s.offset, buf)
+            outcomes["ok"] += 1
+        except mov.Error:
+            outcomes["error"] += 1
+    assert outcomes["ok"] > 0 and outcomes["error"] > 0, outcomes
