@@ -573,3 +573,49 @@ def test_develop_runs_on_a_decoded_frame(impl):
     img = impl.develop(raw, impl.params(raw.header, f.quantizer()), 1, False)
     assert img.size == 48 * 32 * 3
     assert np.all(np.isfinite(img)) and np.all(img <= 1.0)
+
+
+def _error_code(fn, *args):
+    try:
+        fn(*args)
+    except (P.Error, O.OracleError) as e:
+        return e.code, getattr(e, "fields", None)
+    return 0, None
+
+
+def test_corrupted_packets_parse_like_the_oracle():
+    # Byte changes and truncations in the prefix, the header and the tile
+    # size table: the library's host parse (header, grid, size-table walk)
+    # gives the oracle's result, the same error or the same frame, and never
+    # reads out of bounds.
+    import random
+
+    rng = random.Random(3)
+    srng = S.Rng(5)
+    bases = [S.random_frame(spec, srng) for spec in S.specs(srng)[:6]]
+    for trial in range(800):
+        pkt = bytearray(rng.choice(bases))
+        n = P.header_len(bytes(pkt)) if len(pkt) > 10 else 10
+        for _ in range(rng.randrange(1, 4)):
+            kind = rng.randrange(3)
+            if kind == 0 and len(pkt) > 1:
+                # a byte of the prefix, header or size table
+                pkt[rng.randrange(min(len(pkt), n + 64))] = rng.randrange(256)
+            elif kind == 1 and len(pkt) > 1:
+                del pkt[rng.randrange(1, len(pkt)):]
+            elif len(pkt) > 12:
+                at = rng.randrange(0, min(len(pkt) - 2, n + 64))
+                pkt[at:at + 2] = struct.pack(">H", rng.choice([0, 1, 0xFFFF, 0x8000, len(pkt) & 0xFFFF]))
+        p = bytes(pkt)
+        got_code, got_fields = _error_code(P.parse_frame, p)
+        try:
+            want = O.parse_frame(p)
+            want_code = 0
+        except O.OracleError as e:
+            want, want_code = None, e.code
+        assert got_code == want_code, (trial, got_code, want_code)
+        if want_code == 0:
+            f = P.parse_frame(p)
+            oh, off, ln, tpr, rows, mq = want
+            assert (f.ntiles, f.tiles_per_row, f.tile_rows, f.max_qscale) == (len(off), tpr, rows, mq)
+        assert _error_code(P.parse_header, p)[0] == _error_code(O.parse_header, p)[0]
