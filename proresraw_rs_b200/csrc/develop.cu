@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 
 #include "device_common.cuh"
@@ -492,21 +493,28 @@ template <bool PRE>
 cudaError_t develop_reserve(uint32_t ctas, size_t* bytes) {
     *bytes = 0;
     if (ctas == 0) return cudaSuccess;
-    static size_t cache[2][17] = {};
-    static bool known[2][17] = {};
-    if (ctas <= 16 && known[PRE][ctas]) {
-        *bytes = cache[PRE][ctas];
-        return cudaSuccess;
-    }
+    // Per device and cap: the pad found, plus one (0: not yet found). The
+    // attribute below is set on the device the first time.
+    static std::atomic<uint32_t> cache[kMaxDevices][17];
     int dev = 0, per_sm = 0, per_block = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices || ctas > 16) return cudaErrorInvalidValue;
+    const uint32_t known = cache[dev][ctas].load(std::memory_order_acquire);
+    if (known) {
+        *bytes = known - 1;
+        return cudaSuccess;
+    }
+    cudaFuncAttributes fa;
+    e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_develop<PRE>);
+    if (e != cudaSuccess) return e;
+    const size_t fixed = fa.sharedSizeBytes;  // the kernel's static shared memory
     // A block's static plus dynamic shared memory above 48 KB needs the
     // opt-in limit.
     e = cudaFuncSetAttribute(k_develop<PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(std::min<size_t>(size_t(per_block) - sizeof(DevShared), size_t(per_sm))));
+                             int(std::min<size_t>(size_t(per_block) - fixed, size_t(per_sm))));
     if (e != cudaSuccess) return e;
     const size_t step = 1024;
     size_t pad = 0;
@@ -514,13 +522,10 @@ cudaError_t develop_reserve(uint32_t ctas, size_t* bytes) {
         int n = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_develop<PRE>, kDevThreads, pad);
         if (e != cudaSuccess) return e;
-        if (n <= int(ctas) || pad + sizeof(DevShared) + step > size_t(per_block)) break;
+        if (n <= int(ctas) || pad + fixed + step > size_t(per_block)) break;
         pad += step;
     }
-    if (ctas <= 16) {
-        cache[PRE][ctas] = pad;
-        known[PRE][ctas] = true;
-    }
+    cache[dev][ctas].store(uint32_t(pad) + 1, std::memory_order_release);
     *bytes = pad;
     return cudaSuccess;
 }

@@ -144,6 +144,8 @@ struct DevelopDesc {
 };
 
 constexpr int kDevelopTile = 32;
+// Devices a process may use with the library's per-device launch caches.
+constexpr int kMaxDevices = 64;
 
 // Argument checks and kernel descriptor of develop_into / develop_planar_into
 // (api.cu), and output_matrix (src/demosaic.rs:138-153).

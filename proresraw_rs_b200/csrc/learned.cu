@@ -52,6 +52,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -547,15 +548,21 @@ using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-cudaError_t encode_window_map(CUtensorMap* map, const void* x, int c8, int H, int W, int images) {
-    static EncodeTiledFn fn = nullptr;
-    if (!fn) {
+// The driver's encoder, looked up once (a thread-safe static initializer);
+// null when the runtime cannot find it.
+EncodeTiledFn encode_tiled() {
+    static const EncodeTiledFn fn = [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
-        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return e != cudaSuccess ? e : cudaErrorUnknown;
-        fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
+        return e == cudaSuccess && q == cudaDriverEntryPointSuccess ? reinterpret_cast<EncodeTiledFn>(p) : nullptr;
+    }();
+    return fn;
+}
+
+cudaError_t encode_window_map(CUtensorMap* map, const void* x, int c8, int H, int W, int images) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn) return cudaErrorUnknown;
     // The activation tensor as 3-D bf16: a row of one chunk (8 channels x W
     // pixels, contiguous), y, and (image, chunk) planes; the half-window box
     // is HX pixels of a row, WY rows, one image's chunks.
@@ -576,15 +583,19 @@ cudaError_t conv_launch(const ConvArgs& a, const RgbOut& o, int images, cudaStre
     // two CTAs share an SM: two CTAs' 2 x 4 x COUT accumulator columns fit
     // in its 512, and a third CTA's allocation would wait for one of them.
     constexpr int smem = std::max(((C::W_BYTES + 127) & ~127) + kStages * ((C::WIN_BYTES + 127) & ~127), 80 * 1024);
-    static int sms = 0;  // per process: the attribute and SM count of the first device used
+    // The shared-memory limit and the SM count, set and read once per device
+    // (kept per device in atomics: contexts on several threads launch too).
+    static std::atomic<int> sms_of[kMaxDevices];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    int sms = sms_of[dev].load(std::memory_order_acquire);
     if (sms == 0) {
-        cudaError_t e = cudaFuncSetAttribute(k_sg_conv<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             smem);
-        if (e != cudaSuccess) return e;
-        int dev = 0;
-        e = cudaGetDevice(&dev);
+        e = cudaFuncSetAttribute(k_sg_conv<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
+        sms_of[dev].store(sms, std::memory_order_release);
     }
     alignas(64) CUtensorMap map;
     const cudaError_t em = encode_window_map(&map, a.x, C::C8, a.H, a.W, images);
@@ -1460,14 +1471,8 @@ namespace prr {
 // apart (a multiple of 16), boxes of box_w x box_h, no swizzle.
 cudaError_t encode_u16_map_2d(CUtensorMap* map, const void* base, uint64_t width, uint64_t height,
                               uint64_t row_bytes, uint32_t box_w, uint32_t box_h) {
-    static sg::EncodeTiledFn fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        const cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q);
-        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !p) return e != cudaSuccess ? e : cudaErrorUnknown;
-        fn = reinterpret_cast<sg::EncodeTiledFn>(p);
-    }
+    const sg::EncodeTiledFn fn = sg::encode_tiled();
+    if (!fn) return cudaErrorUnknown;
     const cuuint64_t dims[2] = {width, height};
     const cuuint64_t strides[1] = {row_bytes};
     const cuuint32_t box[2] = {box_w, box_h};

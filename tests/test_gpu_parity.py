@@ -291,3 +291,17 @@ def test_host_buffer_develop_matches():
     assert rc == 0
     for c, plane in enumerate((r, g, b)):
         assert np.array_equal(plane.view(np.uint32), want[c].view(np.uint32))
+
+
+@pytest.mark.parametrize("ctas", [1, 2, 3])
+def test_develop_under_an_occupancy_cap_is_unchanged(ctas):
+    # prr_develop_set_occupancy reserves shared memory per CTA so that at
+    # most `ctas` develop CTAs share an SM; the output stays the oracle's.
+    pkt = encoded(700, 300, pattern=3, alignment=4, qscale=45, sigma=24.0, seed=ctas)
+    ctx = P.context()
+    assert _lib.lib().prr_develop_set_occupancy(ctx, ctas) == 0
+    try:
+        develop_compare(pkt, stages=(2,))
+    finally:
+        assert _lib.lib().prr_develop_set_occupancy(ctx, 0) == 0
+    assert _lib.lib().prr_develop_set_occupancy(ctx, 17) == _lib.ERR_INVALID
