@@ -245,7 +245,7 @@ typedef struct prr_job {
 /* Launch shape of the batch kernel, per bucket of batches. */
 typedef struct prr_batch_config {
     uint32_t ctas_per_sm;  /* persistent CTAs per SM; 0: as many as fit */
-    uint32_t stage_bytes;  /* packet bytes a 64-tile chunk stages in shared memory:
+    uint32_t stage_bytes;  /* packet bytes a 128-tile entropy item stages in shared memory:
                               a multiple of 16, at most 98304 */
     uint32_t use_graph;    /* replay a CUDA graph captured for the bucket */
     uint32_t pad;

@@ -534,7 +534,7 @@ int prr_batch_tune(prr_ctx* c, prr_job* jobs, size_t n, uint32_t reps, prr_batch
     PRR_TRY(prr_batch_bucket(c, jobs, n, &bucket));
     prr_batch_config win = default_config();
     float win_ms = 1e30f;
-    static const uint32_t stages[] = {16 * 1024, 32 * 1024, 48 * 1024, 64 * 1024};
+    static const uint32_t stages[] = {16 * 1024, 32 * 1024, 48 * 1024, 64 * 1024, 96 * 1024};
     for (uint32_t stage : stages) {
         int max_per_sm = 0;
         PRR_TRY(c->cuda(batch_max_ctas_per_sm(stage, &max_per_sm)));

@@ -840,16 +840,12 @@ __device__ __forceinline__ StreamJob stream_job(const FrameDesc& d, int greens, 
 // Entropy-decode the streams of tiles [chunk * blockDim.x / 4, ...) of a
 // frame, one stream per thread. `stage` holds stage_bytes + 16 bytes of
 // shared memory; the chunk's packet span is copied there when it fits.
-// With SORT, the threads take the chunk's streams in order of their byte
-// length, so that the 32 lanes of a warp decode streams of about the same
-// number of symbols and stay busy together (a warp loops until its longest
-// stream ends). Ends with the CTA's threads at different points (no
-// barrier).
-template <uint32_t LC, bool SORT>
+// Ends with the CTA's threads at different points (no barrier).
+template <uint32_t LC>
 __device__ __forceinline__ void entropy_chunk(const EntropyTables& T, uint32_t* stage, uint32_t stage_bytes,
                                               const FrameDesc& d, int greens,
                                               const uint32_t* __restrict__ tile_off, prr_dev_status* st,
-                                              uint32_t chunk, uint32_t* keys = nullptr) {
+                                              uint32_t chunk) {
     // The chunk's tiles [t0, t1) occupy bytes [tile_off[t0], tile_off[t1]).
     const uint32_t t0 = chunk * (blockDim.x / 4);
     const uint32_t t1 = min(t0 + blockDim.x / 4, d.ntiles);
@@ -865,32 +861,8 @@ __device__ __forceinline__ void entropy_chunk(const EntropyTables& T, uint32_t* 
             dst[i] = make_uint4(bswap32(v.x), bswap32(v.y), bswap32(v.z), bswap32(v.w));
         }
     }
-    StreamJob job = stream_job<LC>(d, greens, tile_off, chunk * blockDim.x + threadIdx.x);
-    if (SORT) {
-        // Bitonic sort of (length << 9 | thread) over the block (a power of
-        // two, at most 512 threads) in `keys` (shared, a word per thread);
-        // thread i then takes the stream of the i-th key.
-        keys[threadIdx.x] = (job.valid ? (min(job.slen, 0x7FFFFFu) << 9) : 0u) | threadIdx.x;
-        __syncthreads();
-        const uint32_t n = blockDim.x, i = threadIdx.x;
-        for (uint32_t k = 2; k <= n; k <<= 1) {
-            for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
-                const uint32_t p = i ^ jj;
-                if (p > i) {
-                    const uint32_t a = keys[i], b = keys[p];
-                    if ((a > b) == ((i & k) == 0)) {
-                        keys[i] = b;
-                        keys[p] = a;
-                    }
-                }
-                __syncthreads();
-            }
-        }
-        const uint32_t src = keys[i] & 511;
-        if (src != i) job = stream_job<LC>(d, greens, tile_off, chunk * blockDim.x + src);
-    } else {
-        __syncthreads();
-    }
+    __syncthreads();
+    const StreamJob job = stream_job<LC>(d, greens, tile_off, chunk * blockDim.x + threadIdx.x);
     if (!job.valid) return;
     uint32_t* list = d.pairs + stream_list_base(d, job.trow, job.x, job.log2, job.s, LC);
     bool revisited = false, ok = true;
@@ -910,7 +882,7 @@ __global__ void __launch_bounds__(128) k_entropy(FrameDesc d, int greens, const 
     load_tables(&CT);
     __syncthreads();
     build_entropy_tables(T, CT);
-    entropy_chunk<LC, false>(T, stage, kStageBytes, d, greens, tile_off, st, blockIdx.x);
+    entropy_chunk<LC>(T, stage, kStageBytes, d, greens, tile_off, st, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1046,11 +1018,67 @@ __device__ __forceinline__ uint32_t batch_frame_of(const BatchDesc& b, uint32_t 
 
 // The batch kernel's work items as separate functions, so that each gets
 // the registers it needs on its own instead of the sum of all of them.
+// An entropy item of the batch kernel: the 2 x blockDim.x streams of
+// kBatchTilesPerChunk tiles. The item's packet span is staged when it fits;
+// the streams are sorted by byte length (bitonic, two keys a thread) and
+// thread i decodes the i-th shortest and the i-th longest, so every lane
+// has about the same number of symbols to decode and the CTA's warps reach
+// the item's closing barrier together.
 template <uint32_t LC>
 __device__ __noinline__ void batch_entropy(const EntropyTables& T, uint32_t* stage, uint32_t stage_bytes,
                                            const FrameDesc& d, int greens, const uint32_t* tile_off,
-                                           prr_dev_status* st, uint32_t chunk, uint32_t* keys) {
-    entropy_chunk<LC, true>(T, stage, stage_bytes, d, greens, tile_off, st, chunk, keys);
+                                           prr_dev_status* st, uint32_t item, uint32_t* keys) {
+    const uint32_t n = 2 * blockDim.x;  // streams of the item (a power of two, at most 1024)
+    const uint32_t g0 = item * n;
+    const uint32_t t0 = g0 / 4;
+    const uint32_t t1 = min(t0 + n / 4, d.ntiles);
+    const uint32_t hi = min(tile_off[t1], d.len);
+    const uint32_t lo = min(tile_off[t0], hi);
+    const uint32_t base = lo & ~15u, top = (hi + 15) & ~15u;  // within the padded packet buffer
+    const bool staged = top - base <= stage_bytes;
+    if (staged) {
+        const uint4* src = reinterpret_cast<const uint4*>(d.words) + base / 16;
+        uint4* dst = reinterpret_cast<uint4*>(stage);
+        for (uint32_t i = threadIdx.x; i < (top - base) / 16; i += blockDim.x) {
+            const uint4 v = __ldg(src + i);
+            dst[i] = make_uint4(bswap32(v.x), bswap32(v.y), bswap32(v.z), bswap32(v.w));
+        }
+    }
+    for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
+        const StreamJob jb = stream_job<LC>(d, greens, tile_off, g0 + e);
+        keys[e] = (jb.valid ? (min(jb.slen, 0x3FFFFFu) << 10) : 0u) | e;
+    }
+    __syncthreads();
+    for (uint32_t k = 2; k <= n; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
+                const uint32_t p = e ^ j;
+                if (p > e) {
+                    const uint32_t a = keys[e], b = keys[p];
+                    if ((a > b) == ((e & k) == 0)) {
+                        keys[e] = b;
+                        keys[p] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const uint32_t i = threadIdx.x;
+    const uint32_t mine[2] = {keys[i] & 1023, keys[n - 1 - i] & 1023};
+#pragma unroll 1
+    for (int q = 0; q < 2; q++) {
+        const StreamJob jb = stream_job<LC>(d, greens, tile_off, g0 + mine[q]);
+        if (!jb.valid) continue;
+        uint32_t* list = d.pairs + stream_list_base(d, jb.trow, jb.x, jb.log2, jb.s, LC);
+        bool revisited = false, ok = true;
+        const uint32_t cnt =
+            staged ? entropy_events<LC>(StagedWords{stage, base >> 2}, jb.soff, jb.slen, jb.log2, T, list, revisited,
+                                        ok)
+                   : entropy_events<LC>(PacketWords{d.words}, jb.soff, jb.slen, jb.log2, T, list, revisited, ok);
+        if (!ok) atomicOr(&st->error, 1u);
+        d.counts[jb.g] = revisited ? 0x80000000u : cnt;
+    }
 }
 template <int IDCT>
 __device__ __noinline__ void batch_full(SegShared& S, const FrameDesc& d, uint32_t seg, uint32_t trow,
@@ -1076,7 +1104,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
     __shared__ EntropyTables T;
     __shared__ FrameDesc fd;
     __shared__ uint32_t s_item, s_frame, s_epoch, s_ok;
-    __shared__ uint32_t keys[kBatchThreads];  // the entropy chunks' stream order
+    __shared__ uint32_t keys[2 * kBatchThreads];  // the entropy items' stream order
     const uint32_t tid = threadIdx.x;
     load_tables(&S.T);
     if (tid == 0) s_epoch = b.q->epoch;

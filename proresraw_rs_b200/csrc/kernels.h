@@ -97,7 +97,8 @@ struct BatchDesc {
 };
 
 constexpr uint32_t kBatchThreads = 256;
-constexpr uint32_t kBatchTilesPerChunk = kBatchThreads / 4;
+// Tiles of an entropy item: two streams a thread (four streams a tile).
+constexpr uint32_t kBatchTilesPerChunk = kBatchThreads / 2;
 constexpr uint32_t kBatchMaxStageBytes = 96 * 1024;
 // Dynamic shared memory of the batch kernel for a packet stage of
 // stage_bytes (<= kBatchMaxStageBytes), and the CTAs per SM that fit.
