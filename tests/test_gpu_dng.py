@@ -108,3 +108,33 @@ def test_write_into_a_buffer():
     assert e.value.code == P._lib.ERR_BUFFER
     big = bytearray(len(want))
     assert D.write_into(frame, big, D.ClipInfo(make="A")) == len(want) and bytes(big) == want
+
+
+def test_device_output_entry_point():
+    # prr_lj92_encode: the streams packed in a device buffer with their
+    # offsets on the device, as the host variant returns them; a buffer
+    # under the worst-case bound is refused before any launch.
+    import ctypes as C
+
+    from proresraw_rs_b200 import _lib
+
+    rng = np.random.default_rng(4)
+    w, h, t = 520, 300, 256
+    img = rng.integers(0, 1 << 14, w * h, dtype=np.uint16)
+    dimg = device(img, h, w)
+    L = _lib.lib()
+    ctx = P.context()
+    n = -(-w // t) * -(-h // t)
+    cap = n * int(L.prr_lj92_tile_bound(t))
+    out = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    offs = torch.zeros(n + 1, dtype=torch.int64, device="cuda")
+    assert L.prr_lj92_encode(ctx, dimg.data_ptr(), w, h, w, t, out.data_ptr(), cap, offs.data_ptr()) == 0
+    torch.cuda.synchronize()
+    o = offs.cpu().numpy()
+    data = out[: int(o[-1])].cpu().numpy().tobytes()
+    got = [data[int(o[i]):int(o[i + 1])] for i in range(n)]
+    assert got == O.lj92_tiles(img, w, h, tile=t)
+    assert L.prr_lj92_encode(ctx, dimg.data_ptr(), w, h, w, t, out.data_ptr(), cap - 1,
+                             offs.data_ptr()) == _lib.ERR_BUFFER
+    assert L.prr_lj92_encode(ctx, dimg.data_ptr(), 1, h, w, t, out.data_ptr(), cap,
+                             offs.data_ptr()) == _lib.ERR_INVALID
