@@ -127,6 +127,138 @@ __device__ __forceinline__ float estimate2(float xu, float xv, float gu, float g
     return fma_(sub(mean_mid, mean_x), weight, mean_x);
 }
 
+// Packed pairs of f32 (sm_100 f32x2 arithmetic): each lane is rounded as the
+// scalar operation rounds it, so two sites computed as the lanes of one pair
+// give the scalar results bit for bit in half the issued instructions.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    unsigned long long x, y, r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "f"(a.x), "f"(a.y));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(y) : "f"(b.x), "f"(b.y));
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(x), "l"(y));
+    float2 o;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+    return o;
+}
+__device__ __forceinline__ float2 bc(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 dot4x2(float2 a0, float2 a1, float2 a2, float2 a3, float2 b0, float2 b1, float2 b2,
+                                         float2 b3) {
+    return fma2(a3, b3, fma2(a2, b2, fma2(a0, b0, mul2(a1, b1))));
+}
+// variance() of two values, one a lane.
+__device__ __forceinline__ float2 variance2(float2 v, float off, const Noise& n) {
+    const float2 t = add2(bc(off), v);
+    const float2 m = mul2(bc(n.a), mul2(t, t));
+    return add2(bc(n.c), make_float2(fmaxf(n.b, m.x), fmaxf(n.b, m.y)));
+}
+
+// estimate() of two sites, one a lane (src/demosaic.rs:572-604). A lane
+// whose test fails returns its mean; its divisions are skipped.
+__device__ __forceinline__ float2 estimate_x2(const float2* xx, const float2* gg, const float2* var_x,
+                                              const float2* sx, const float2* sg, float2 cg, float2 cs) {
+    const float2 q = bc(0.25f);
+    const float2 mean_x = dot4x2(xx[0], xx[1], xx[2], xx[3], q, q, q, q);
+    bool okx = cs.x < cg.x, oky = cs.y < cg.y;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        okx &= (sx[i].x < xx[i].x) & (sg[i].x < gg[i].x);
+        oky &= (sx[i].y < xx[i].y) & (sg[i].y < gg[i].y);
+    }
+    if (!(okx | oky)) return mean_x;
+    // The variance and deviation terms first, so that the neighbours'
+    // values die as the divisions consume them.
+    const float2 dx0 = sub2(xx[0], mean_x), dx1 = sub2(xx[1], mean_x), dx2 = sub2(xx[2], mean_x),
+                 dx3 = sub2(xx[3], mean_x);
+    // dot4 of the variances with ones: fma(v, 1, s) is add(v, s) exactly.
+    const float2 vsum = add2(var_x[3], add2(var_x[2], add2(var_x[0], var_x[1])));
+    const float2 a = fma2(vsum, bc(0.75f), dot4x2(dx0, dx1, dx2, dx3, dx0, dx1, dx2, dx3));
+    const float2 k1 = sub2(cg, cs), k2 = add2(cs, cg);
+    float2 mid[4], ml[4], hm[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float2 nlo = mul2(k1, sub2(xx[i], sx[i])), dlo = add2(sg[i], gg[i]);
+        const float2 nmid = mul2(cg, xx[i]);
+        const float2 nhi = mul2(k2, add2(sx[i], xx[i])), dhi = sub2(gg[i], sg[i]);
+        // A failing lane keeps its numerators (never used).
+        float2 lo = nlo, md = nmid, hi = nhi;
+        if (okx) {
+            lo.x = dv(nlo.x, dlo.x);
+            md.x = dv(nmid.x, gg[i].x);
+            hi.x = dv(nhi.x, dhi.x);
+        }
+        if (oky) {
+            lo.y = dv(nlo.y, dlo.y);
+            md.y = dv(nmid.y, gg[i].y);
+            hi.y = dv(nhi.y, dhi.y);
+        }
+        mid[i] = md;
+        ml[i] = sub2(md, lo);
+        hm[i] = sub2(hi, md);
+    }
+    const float2 spread = dot4x2(ml[0], ml[1], ml[2], ml[3], hm[0], hm[1], hm[2], hm[3]);
+    const float2 mean_mid = dot4x2(mid[0], mid[1], mid[2], mid[3], q, q, q, q);
+    const float2 dm0 = sub2(mid[0], mean_mid), dm1 = sub2(mid[1], mean_mid), dm2 = sub2(mid[2], mean_mid),
+                 dm3 = sub2(mid[3], mean_mid);
+    const float2 b = fma2(spread, bc(0.75f), dot4x2(dm0, dm1, dm2, dm3, dm0, dm1, dm2, dm3));
+    const float2 den = add2(b, a);
+    float2 weight = a;
+    if (okx) weight.x = dv(a.x, den.x);
+    if (oky) weight.y = dv(a.y, den.y);
+    const float2 r = fma2(sub2(mean_mid, mean_x), weight, mean_x);
+    return make_float2(okx ? r.x : mean_x.x, oky ? r.y : mean_x.y);
+}
+
+// estimate2() of two (u, v) neighbour pairs, one a lane.
+__device__ __forceinline__ float2 estimate2_x2(float2 xu, float2 xv, float2 gu, float2 gv, float2 vu, float2 vv,
+                                               float2 su, float2 sv, float2 tu, float2 tv, float2 cg, float2 cs) {
+    const float2 q = bc(0.25f);
+    const float2 mean_x = fma2(xv, q, fma2(xu, q, fma2(xu, q, mul2(xv, q))));
+    const bool okx = (cs.x < cg.x) & (su.x < xu.x) & (tu.x < gu.x) & (sv.x < xv.x) & (tv.x < gv.x);
+    const bool oky = (cs.y < cg.y) & (su.y < xu.y) & (tu.y < gu.y) & (sv.y < xv.y) & (tv.y < gv.y);
+    if (!(okx | oky)) return mean_x;
+    const float2 dx_u = sub2(xu, mean_x), dx_v = sub2(xv, mean_x);
+    const float2 vsum = add2(vv, add2(vu, add2(vu, vv)));
+    const float2 a = fma2(vsum, bc(0.75f), fma2(dx_v, dx_v, fma2(dx_u, dx_u, fma2(dx_u, dx_u, mul2(dx_v, dx_v)))));
+    const float2 k1 = sub2(cg, cs), k2 = add2(cs, cg);
+    const float2 nlo_u = mul2(k1, sub2(xu, su)), nlo_v = mul2(k1, sub2(xv, sv));
+    const float2 dlo_u = add2(tu, gu), dlo_v = add2(tv, gv);
+    const float2 nmid_u = mul2(cg, xu), nmid_v = mul2(cg, xv);
+    const float2 nhi_u = mul2(k2, add2(su, xu)), nhi_v = mul2(k2, add2(sv, xv));
+    const float2 dhi_u = sub2(gu, tu), dhi_v = sub2(gv, tv);
+    // A failing lane keeps its numerators (never used).
+    float2 lo_u = nlo_u, lo_v = nlo_v, mid_u = nmid_u, mid_v = nmid_v, hi_u = nhi_u, hi_v = nhi_v;
+    if (okx) {
+        lo_u.x = dv(nlo_u.x, dlo_u.x);
+        lo_v.x = dv(nlo_v.x, dlo_v.x);
+        mid_u.x = dv(nmid_u.x, gu.x);
+        mid_v.x = dv(nmid_v.x, gv.x);
+        hi_u.x = dv(nhi_u.x, dhi_u.x);
+        hi_v.x = dv(nhi_v.x, dhi_v.x);
+    }
+    if (oky) {
+        lo_u.y = dv(nlo_u.y, dlo_u.y);
+        lo_v.y = dv(nlo_v.y, dlo_v.y);
+        mid_u.y = dv(nmid_u.y, gu.y);
+        mid_v.y = dv(nmid_v.y, gv.y);
+        hi_u.y = dv(nhi_u.y, dhi_u.y);
+        hi_v.y = dv(nhi_v.y, dhi_v.y);
+    }
+    const float2 ml_u = sub2(mid_u, lo_u), ml_v = sub2(mid_v, lo_v);
+    const float2 hm_u = sub2(hi_u, mid_u), hm_v = sub2(hi_v, mid_v);
+    const float2 spread = fma2(ml_v, hm_v, fma2(ml_u, hm_u, fma2(ml_u, hm_u, mul2(ml_v, hm_v))));
+    const float2 mean_mid = fma2(mid_v, q, fma2(mid_u, q, fma2(mid_u, q, mul2(mid_v, q))));
+    const float2 dm_u = sub2(mid_u, mean_mid), dm_v = sub2(mid_v, mean_mid);
+    const float2 b = fma2(spread, bc(0.75f), fma2(dm_v, dm_v, fma2(dm_u, dm_u, fma2(dm_u, dm_u, mul2(dm_v, dm_v)))));
+    const float2 den = add2(b, a);
+    float2 weight = a;
+    if (okx) weight.x = dv(a.x, den.x);
+    if (oky) weight.y = dv(a.y, den.y);
+    const float2 r = fma2(sub2(mean_mid, mean_x), weight, mean_x);
+    return make_float2(okx ? r.x : mean_x.x, oky ? r.y : mean_x.y);
+}
+
 constexpr int TW = 32, TH = 32;           // output tile
 constexpr int NW = TW + 6, NH = TH + 6;   // normalized values, 3-sensel halo
 constexpr int GW = TW + 2, GH = TH + 2;   // green-pass region, 1-sensel halo
@@ -182,6 +314,97 @@ struct DevShared {
     uint32_t c0[8], cd[8];
 };
 
+// White balance, clip and output matrix of a row's two sites as the lanes
+// of pairs (src/demosaic.rs:682-720).
+__device__ __forceinline__ void finish_x2(float2 r, float2 g, float2 b, const DevelopDesc& d, float2* out) {
+    float2 rr = mul2(r, bc(d.wb[0]));
+    float2 bb = mul2(b, bc(d.wb[1]));
+    rr = make_float2(fminf(rr.x, 1.0f), fminf(rr.y, 1.0f));
+    float2 gg = make_float2(fminf(g.x, 1.0f), fminf(g.y, 1.0f));
+    bb = make_float2(fminf(bb.x, 1.0f), fminf(bb.y, 1.0f));
+    if (d.has_matrix) {
+        const float2 m0 = fma2(bb, bc(d.m[2]), fma2(rr, bc(d.m[0]), mul2(gg, bc(d.m[1]))));
+        const float2 m1 = fma2(bb, bc(d.m[5]), fma2(rr, bc(d.m[3]), mul2(gg, bc(d.m[4]))));
+        const float2 m2 = fma2(bb, bc(d.m[8]), fma2(rr, bc(d.m[6]), mul2(gg, bc(d.m[7]))));
+        rr = m0;
+        gg = m1;
+        bb = m2;
+    }
+    out[0] = rr;
+    out[1] = gg;
+    out[2] = bb;
+}
+
+// The chroma pass of a quad whose neighbours all lie inside the tile's
+// green-pass region and the picture (tiles clear of the edges), every
+// neighbour at a fixed offset. A is the column of the quad's red or blue
+// site in its first row; the other one sits at (1, 1 - A). The four
+// estimates of a quad run two to a pair: the red/blue sites' diagonal
+// estimates (src/demosaic.rs:662-669) as the lanes of one pair, each green
+// site's horizontal and vertical estimates (src/demosaic.rs:670-680) as the
+// lanes of one pair. Returns per quad row the (r, g, b) pairs of its sites.
+template <int A>
+__device__ __forceinline__ void chroma_quad(const DevShared& S, int gyb, int gxb, bool red0, const DevelopDesc& d,
+                                            float2 (&out)[2][3]) {
+    // Region site of the quad offset (dy, dx).
+    auto idx = [&](int dy, int dx) { return (gyb + dy) * GW + gxb + dx; };
+    const float* rb = &S.rb[0][0];
+    const float* gr = &S.gr[0][0];
+    const float* vx = &S.vx[0][0];
+    const float* sx = &S.sx[0][0];
+    const float* sg = &S.sg[0][0];
+    // The diagonal neighbours, in estimate() order (up-left, down-left,
+    // up-right, down-right), of the site (0, A) and of the site (1, 1 - A).
+    const int pn[4] = {idx(-1, A - 1), idx(1, A - 1), idx(-1, A + 1), idx(1, A + 1)};
+    const int qn[4] = {idx(0, -A), idx(2, -A), idx(0, 2 - A), idx(2, 2 - A)};
+    // Two (u, v) neighbour pairs as lanes: lane x (ux, vx_), lane y (uy, vy).
+    auto pair2 = [&](int ux, int vx_, int uy, int vy, float2 cg, float2 cs) {
+        return estimate2_x2(make_float2(rb[ux], rb[uy]), make_float2(rb[vx_], rb[vy]), make_float2(gr[ux], gr[uy]),
+                            make_float2(gr[vx_], gr[vy]), make_float2(vx[ux], vx[uy]), make_float2(vx[vx_], vx[vy]),
+                            make_float2(sx[ux], sx[uy]), make_float2(sx[vx_], sx[vy]), make_float2(sg[ux], sg[uy]),
+                            make_float2(sg[vx_], sg[vy]), cg, cs);
+    };
+    // Green site (0, 1 - A): lane x its horizontal neighbours qn[0], qn[2],
+    // lane y its vertical ones pn[2], pn[3] (A = 0) or pn[0], pn[1] (A = 1).
+    const int g0 = idx(0, 1 - A);
+    const float gc_0 = gr[g0];
+    const float2 e0 = pair2(qn[0], qn[2], pn[A == 0 ? 2 : 0], pn[A == 0 ? 3 : 1], bc(gc_0), bc(sg[g0]));
+    // Green site (1, A): horizontal neighbours pn[1], pn[3]; vertical ones
+    // qn[0], qn[1] (A = 0) or qn[2], qn[3] (A = 1).
+    const int g1 = idx(1, A);
+    const float gc_1 = gr[g1];
+    const float2 e1 = pair2(pn[1], pn[3], qn[A == 0 ? 0 : 2], qn[A == 0 ? 1 : 3], bc(gc_1), bc(sg[g1]));
+    // The red/blue sites' diagonal estimates: lane x the site (0, A), lane y
+    // the site (1, 1 - A).
+    float2 X[4], G[4], V[4], SX[4], SG[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        X[i] = make_float2(rb[pn[i]], rb[qn[i]]);
+        G[i] = make_float2(gr[pn[i]], gr[qn[i]]);
+        V[i] = make_float2(vx[pn[i]], vx[qn[i]]);
+        SX[i] = make_float2(sx[pn[i]], sx[qn[i]]);
+        SG[i] = make_float2(sg[pn[i]], sg[qn[i]]);
+    }
+    const int ca = idx(0, A), cb = idx(1, 1 - A);
+    const float gc_a = gr[ca], gc_b = gr[cb];
+    const float2 e = estimate_x2(X, G, V, SX, SG, make_float2(gc_a, gc_b), make_float2(sg[ca], sg[cb]));
+    const float c_a = rb[ca], c_b = rb[cb];
+    // Site (0, A) lies on the first row, (1, 1 - A) on the second; on a red
+    // row r is the site's own value, or for a green site the horizontal
+    // estimate (src/demosaic.rs:662-688).
+    const float r_a = red0 ? c_a : e.x, b_a = red0 ? e.x : c_a;
+    const float r_b = red0 ? e.y : c_b, b_b = red0 ? c_b : e.y;
+    const float r_g0 = red0 ? e0.x : e0.y, b_g0 = red0 ? e0.y : e0.x;
+    const float r_g1 = red0 ? e1.y : e1.x, b_g1 = red0 ? e1.x : e1.y;
+    if (A == 0) {
+        finish_x2(make_float2(r_a, r_g0), make_float2(gc_a, gc_0), make_float2(b_a, b_g0), d, out[0]);
+        finish_x2(make_float2(r_g1, r_b), make_float2(gc_1, gc_b), make_float2(b_g1, b_b), d, out[1]);
+    } else {
+        finish_x2(make_float2(r_g0, r_a), make_float2(gc_0, gc_a), make_float2(b_g0, b_a), d, out[0]);
+        finish_x2(make_float2(r_b, r_g1), make_float2(gc_b, gc_1), make_float2(b_b, b_g1), d, out[1]);
+    }
+}
+
 }  // namespace
 
 // PRE: the green pass reads the per-sensel noise terms staged in shared
@@ -191,8 +414,11 @@ struct DevShared {
 // each neighbour slot holds a sensel of the site type the slot's clip limit
 // assumes (green at distance 1, the centre's colour at distance 2). Frames 2
 // sensels wide or tall keep the direct evaluation.
+// Four CTAs per SM (64 registers a thread): the kernel is bound by
+// instruction issue and loses more to three CTAs' fewer warps than it gains
+// from the registers it would spill less.
 template <bool PRE>
-__global__ void __launch_bounds__(kDevThreads) k_develop(const __grid_constant__ CUtensorMap codes_map,
+__global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constant__ CUtensorMap codes_map,
                                                          DevelopDesc d) {
     __shared__ DevShared S;
     __shared__ __align__(128) uint16_t box[NH][kBoxW];
@@ -253,8 +479,91 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(const __grid_constant__
     // x0 + TW] x [y0 - 1, y0 + TH], so tiles clear of the edges skip it
     // (a branch uniform over the block).
     const bool near_edge = x0 < 3 || x0 + TW + 3 > w || y0 < 3 || y0 + TH + 3 > h;
-    // 2. Green pass on the region: red/blue sites first (the heavy ones),
-    //    17 per region row, then green sites.
+    // 2. Green pass on the region.
+    if (PRE && !near_edge) {
+        // Tiles clear of the edges: no mirror(), every site inside the
+        // picture. Two sites a thread as the lanes of pairs: the red/blue
+        // sites of region quad u (rows 2i and 2i + 1, columns 2j and
+        // 2j + 1; the heavy ones) for u < kQuads, then the green sites of
+        // quad u - kQuads. Lane x is the site of row 2i, lane y that of row
+        // 2i + 1. Region row gy is picture row y0 - 1 + gy, odd for even gy.
+        constexpr int kQuads = (GH / 2) * (GW / 2);
+        const bool phase0 = red_row == 1;
+        const int f0 = phase0 ? red_col : 1 - red_col;  // first green column of row 2i, mod 2
+        const float2 clip = phase0 ? make_float2(d.clip[0], d.clip[1]) : make_float2(d.clip[1], d.clip[0]);
+        for (int u = tid; u < 2 * kQuads; u += kDevThreads) {
+            const bool rbsite = u < kQuads;
+            const int uu = rbsite ? u : u - kQuads;
+            const int i = uu / (GW / 2), j = uu - i * (GW / 2);
+            const int gy0 = 2 * i, gy1 = gy0 + 1;
+            const int gx0 = 2 * j + (rbsite ? 1 - f0 : f0), gx1 = 2 * j + (rbsite ? f0 : 1 - f0);
+            const int ty0 = gy0 + 2, tx0 = gx0 + 2, ty1 = gy1 + 2, tx1 = gx1 + 2;  // nrm coordinates
+            const float2 centre = make_float2(S.nrm[ty0][tx0], S.nrm[ty1][tx1]);
+            float2 rbv = make_float2(0.0f, 0.0f), gv_out = centre;
+            if (rbsite) {
+                const float2 c = make_float2(fminf(centre.x, clip.x), fminf(centre.y, clip.y));
+                const float2 sdc = make_float2(S.gsd[ty0][tx0], S.gsd[ty1][tx1]);
+                const bool condx = c.x > sdc.x, condy = c.y > sdc.y;
+                float2 g[2], e[2];
+#pragma unroll
+                for (int dir = 0; dir < 2; dir++) {
+                    // Neighbours at distance 1 (green) and 2 (the centre's
+                    // colour), in the order of src/demosaic.rs:499-505.
+                    const int oy[4] = {dir ? -1 : 0, dir ? 1 : 0, dir ? -2 : 0, dir ? 2 : 0};
+                    const int ox[4] = {dir ? 0 : -1, dir ? 0 : 1, dir ? 0 : -2, dir ? 0 : 2};
+                    float2 dd[4], sd[4];
+#pragma unroll
+                    for (int n = 0; n < 4; n++) {
+                        const float lx = n < 2 ? 1.0f : clip.x, ly = n < 2 ? 1.0f : clip.y;
+                        dd[n] = make_float2(fminf(S.nrm[ty0 + oy[n]][tx0 + ox[n]], lx),
+                                            fminf(S.nrm[ty1 + oy[n]][tx1 + ox[n]], ly));
+                        sd[n] = make_float2(S.gsd[ty0 + oy[n]][tx0 + ox[n]], S.gsd[ty1 + oy[n]][tx1 + ox[n]]);
+                    }
+                    const float2 sums01 = add2(dd[0], dd[1]), sums23 = add2(dd[2], dd[3]);
+                    float2 ratio = make_float2(0.0f, 0.0f);
+                    if (condx | condy) {
+                        const float2 t0 = add2(mul2(c, bc(2.0f)), sums23);
+                        const float2 t2 = add2(mul2(c, bc(-2.0f)), sums23);
+                        const float2 a = sub2(dd[0], dd[1]), b = sub2(dd[2], dd[3]);
+                        const float2 ab = mul2(a, b), pc = mul2(sub2(dd[2], c), sub2(dd[3], c));
+                        const float2 s01 = add2(sd[0], sd[1]), s23 = add2(sd[2], sd[3]);
+                        const bool anyx = (ab.x > 0.0f) | (pc.x > 0.0f) | (s01.x > fabsf(a.x)) | (s23.x > fabsf(b.x));
+                        const bool anyy = (ab.y > 0.0f) | (pc.y > 0.0f) | (s01.y > fabsf(a.y)) | (s23.y > fabsf(b.y));
+                        const bool allx = (dd[0].x > sd[0].x) & (dd[1].x > sd[1].x) & (dd[2].x > sd[2].x) &
+                                          (dd[3].x > sd[3].x);
+                        const bool ally = (dd[0].y > sd[0].y) & (dd[1].y > sd[1].y) & (dd[2].y > sd[2].y) &
+                                          (dd[3].y > sd[3].y);
+                        const float2 den = mul2(t0, bc(2.0f));
+                        if (condx & anyx & allx) ratio.x = dv(t2.x, den.x);
+                        if (condy & anyy & ally) ratio.y = dv(t2.y, den.y);
+                    }
+                    g[dir] = mul2(mul2(sums01, bc(0.5f)), sub2(bc(1.0f), ratio));
+                    const float2 e0 = sub2(dd[0], g[dir]), e1 = sub2(dd[1], g[dir]), e2 = sub2(dd[2], c),
+                                 e3 = sub2(dd[3], c);
+                    const float2 va = add2(make_float2(S.gvar[ty0 + oy[0]][tx0 + ox[0]], S.gvar[ty1 + oy[0]][tx1 + ox[0]]),
+                                           make_float2(S.gvar[ty0 + oy[1]][tx0 + ox[1]], S.gvar[ty1 + oy[1]][tx1 + ox[1]]));
+                    e[dir] = add2(dot4x2(e0, e1, e2, e3, e0, e1, e2, e3), va);
+                }
+                rbv = c;
+                const float2 num = mul2(sub2(g[0], g[1]), e[1]), den = add2(e[0], e[1]);
+                gv_out = add2(g[1], make_float2(dv(num.x, den.x), dv(num.y, den.y)));
+                const float2 vxx = variance2(rbv, d.chroma_off, nz);
+                S.vx[gy0][gx0] = vxx.x;
+                S.vx[gy1][gx1] = vxx.y;
+                S.sx[gy0][gx0] = rt(vxx.x);
+                S.sx[gy1][gx1] = rt(vxx.y);
+            }
+            const float2 vg = variance2(gv_out, d.chroma_off, nz);
+            S.rb[gy0][gx0] = rbv.x;
+            S.rb[gy1][gx1] = rbv.y;
+            S.gr[gy0][gx0] = gv_out.x;
+            S.gr[gy1][gx1] = gv_out.y;
+            S.sg[gy0][gx0] = rt(vg.x);
+            S.sg[gy1][gx1] = rt(vg.y);
+        }
+    } else
+    // Tiles at the picture edges: one site a thread, red/blue sites first
+    // (the heavy ones), 17 per region row, then green sites.
     for (int k = tid; k < GH * (GW / 2) * 2; k += kDevThreads) {
         const bool rbsite = k < GH * (GW / 2);
         const int kk = rbsite ? k : k - GH * (GW / 2);
@@ -356,6 +665,30 @@ __global__ void __launch_bounds__(kDevThreads) k_develop(const __grid_constant__
     const int qx = tid & 15, qy = tid >> 4;
     const int xb = x0 + 2 * qx, yb = y0 + 2 * qy;
     if (xb >= w || yb >= h) return;
+    if (!near_edge) {
+        // Quad rows start on even picture rows (y0 and 2 * qy are even).
+        const bool red0 = red_row == 0;
+        float2 o2[2][3];
+        if ((red0 ? red_col : 1 - red_col) == 0)
+            chroma_quad<0>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
+        else
+            chroma_quad<1>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
+#pragma unroll
+        for (int dy = 0; dy < 2; dy++) {
+            const size_t p = size_t(yb + dy) * w + xb;
+            if (d.layout == PRR_PLANAR) {
+                *reinterpret_cast<float2*>(d.r + p) = o2[dy][0];
+                *reinterpret_cast<float2*>(d.g + p) = o2[dy][1];
+                *reinterpret_cast<float2*>(d.b + p) = o2[dy][2];
+            } else {
+                float2* o = reinterpret_cast<float2*>(d.r + 3 * p);
+                o[0] = make_float2(o2[dy][0].x, o2[dy][1].x);
+                o[1] = make_float2(o2[dy][2].x, o2[dy][0].y);
+                o[2] = make_float2(o2[dy][1].y, o2[dy][2].y);
+            }
+        }
+        return;
+    }
     float out[2][2][3];
 #pragma unroll
     for (int dy = 0; dy < 2; dy++) {
