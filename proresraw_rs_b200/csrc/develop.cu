@@ -420,7 +420,7 @@ __device__ __forceinline__ void chroma_quad(const DevShared& S, int gyb, int gxb
 template <bool PRE>
 __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constant__ CUtensorMap codes_map,
                                                          DevelopDesc d) {
-    __shared__ DevShared S;
+    __shared__ __align__(16) DevShared S;
     __shared__ __align__(128) uint16_t box[NH][kBoxW];
     __shared__ __align__(8) uint64_t box_bar;
     // Only the tiles a mask selects (the learned develop's fallback tiles).
@@ -455,21 +455,31 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
     const int red_row = d.cfa >> 1, red_col = d.cfa & 1;
     // 1. Normalized values, coordinates clamped to the picture as the green
     //    pass clamps them (src/demosaic.rs:370-375, 499).
-    for (int i = tid; i < NH * NW; i += kDevThreads) {
-        const int ty = i / NW, tx = i - ty * NW;
+    // Two horizontally adjacent values a thread, as the lanes of pairs.
+    for (int i = tid; i < NH * (NW / 2); i += kDevThreads) {
+        const int ty = i / (NW / 2), tx = 2 * (i - ty * (NW / 2));
         const int y = min(max(y0 - 3 + ty, 0), h - 1);
-        const int x = min(max(x0 - 3 + tx, 0), w - 1);
-        const uint32_t code = staged ? uint32_t(box[ty][tx + kBoxX]) : uint32_t(__ldg(d.codes + size_t(y) * d.stride + x));
-        const int32_t lin = int32_t(curve_apply(S.c0, S.cd, code));
-        const float v = mul(d.one_over_range, __int2float_rn(lin - d.black));
-        S.nrm[ty][tx] = v;
+        const int xa = min(max(x0 - 3 + tx, 0), w - 1), xb = min(max(x0 - 2 + tx, 0), w - 1);
+        uint32_t ca, cb;
+        if (staged) {
+            ca = box[ty][tx + kBoxX];
+            cb = box[ty][tx + 1 + kBoxX];
+        } else {
+            const uint16_t* row = d.codes + size_t(y) * d.stride;
+            ca = __ldg(row + xa);
+            cb = __ldg(row + xb);
+        }
+        const int32_t la = int32_t(curve_apply(S.c0, S.cd, ca)), lb = int32_t(curve_apply(S.c0, S.cd, cb));
+        const float2 v = mul2(bc(d.one_over_range), make_float2(__int2float_rn(la - d.black), __int2float_rn(lb - d.black)));
+        *reinterpret_cast<float2*>(&S.nrm[ty][tx]) = v;
         if (PRE) {
             const bool red_line = (y & 1) == red_row;
-            const bool rb = (x & 1) == (red_line ? red_col : 1 - red_col);
-            const float lim = rb ? (red_line ? d.clip[0] : d.clip[1]) : 1.0f;
-            const float var = variance(fminf(v, lim), d.green_off, nz);
-            S.gvar[ty][tx] = var;
-            S.gsd[ty][tx] = rt(var);
+            const int rbc = red_line ? red_col : 1 - red_col;
+            const float rlim = red_line ? d.clip[0] : d.clip[1];
+            const float lima = (xa & 1) == rbc ? rlim : 1.0f, limb = (xb & 1) == rbc ? rlim : 1.0f;
+            const float2 var = variance2(make_float2(fminf(v.x, lima), fminf(v.y, limb)), d.green_off, nz);
+            *reinterpret_cast<float2*>(&S.gvar[ty][tx]) = var;
+            *reinterpret_cast<float2*>(&S.gsd[ty][tx]) = make_float2(rt(var.x), rt(var.y));
         }
     }
     __syncthreads();
