@@ -489,102 +489,15 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
     // x0 + TW] x [y0 - 1, y0 + TH], so tiles clear of the edges skip it
     // (a branch uniform over the block).
     const bool near_edge = x0 < 3 || x0 + TW + 3 > w || y0 < 3 || y0 + TH + 3 > h;
-    // 2. Green pass on the region.
-    if (PRE && !near_edge) {
-        // Tiles clear of the edges: no mirror(), every site inside the
-        // picture. Two sites a thread as the lanes of pairs: the red/blue
-        // sites of region quad u (rows 2i and 2i + 1, columns 2j and
-        // 2j + 1; the heavy ones) for u < kQuads, then the green sites of
-        // quad u - kQuads. Lane x is the site of row 2i, lane y that of row
-        // 2i + 1. Region row gy is picture row y0 - 1 + gy, odd for even gy.
-        constexpr int kQuads = (GH / 2) * (GW / 2);
-        const bool phase0 = red_row == 1;
-        const int f0 = phase0 ? red_col : 1 - red_col;  // first green column of row 2i, mod 2
-        const float2 clip = phase0 ? make_float2(d.clip[0], d.clip[1]) : make_float2(d.clip[1], d.clip[0]);
-        for (int u = tid; u < 2 * kQuads; u += kDevThreads) {
-            const bool rbsite = u < kQuads;
-            const int uu = rbsite ? u : u - kQuads;
-            const int i = uu / (GW / 2), j = uu - i * (GW / 2);
-            const int gy0 = 2 * i, gy1 = gy0 + 1;
-            const int gx0 = 2 * j + (rbsite ? 1 - f0 : f0), gx1 = 2 * j + (rbsite ? f0 : 1 - f0);
-            const int ty0 = gy0 + 2, tx0 = gx0 + 2, ty1 = gy1 + 2, tx1 = gx1 + 2;  // nrm coordinates
-            const float2 centre = make_float2(S.nrm[ty0][tx0], S.nrm[ty1][tx1]);
-            float2 rbv = make_float2(0.0f, 0.0f), gv_out = centre;
-            if (rbsite) {
-                const float2 c = make_float2(fminf(centre.x, clip.x), fminf(centre.y, clip.y));
-                const float2 sdc = make_float2(S.gsd[ty0][tx0], S.gsd[ty1][tx1]);
-                const bool condx = c.x > sdc.x, condy = c.y > sdc.y;
-                float2 g[2], e[2];
-#pragma unroll
-                for (int dir = 0; dir < 2; dir++) {
-                    // Neighbours at distance 1 (green) and 2 (the centre's
-                    // colour), in the order of src/demosaic.rs:499-505.
-                    const int oy[4] = {dir ? -1 : 0, dir ? 1 : 0, dir ? -2 : 0, dir ? 2 : 0};
-                    const int ox[4] = {dir ? 0 : -1, dir ? 0 : 1, dir ? 0 : -2, dir ? 0 : 2};
-                    float2 dd[4], sd[4];
-#pragma unroll
-                    for (int n = 0; n < 4; n++) {
-                        const float lx = n < 2 ? 1.0f : clip.x, ly = n < 2 ? 1.0f : clip.y;
-                        dd[n] = make_float2(fminf(S.nrm[ty0 + oy[n]][tx0 + ox[n]], lx),
-                                            fminf(S.nrm[ty1 + oy[n]][tx1 + ox[n]], ly));
-                        sd[n] = make_float2(S.gsd[ty0 + oy[n]][tx0 + ox[n]], S.gsd[ty1 + oy[n]][tx1 + ox[n]]);
-                    }
-                    const float2 sums01 = add2(dd[0], dd[1]), sums23 = add2(dd[2], dd[3]);
-                    float2 ratio = make_float2(0.0f, 0.0f);
-                    if (condx | condy) {
-                        const float2 t0 = add2(mul2(c, bc(2.0f)), sums23);
-                        const float2 t2 = add2(mul2(c, bc(-2.0f)), sums23);
-                        const float2 a = sub2(dd[0], dd[1]), b = sub2(dd[2], dd[3]);
-                        const float2 ab = mul2(a, b), pc = mul2(sub2(dd[2], c), sub2(dd[3], c));
-                        const float2 s01 = add2(sd[0], sd[1]), s23 = add2(sd[2], sd[3]);
-                        const bool anyx = (ab.x > 0.0f) | (pc.x > 0.0f) | (s01.x > fabsf(a.x)) | (s23.x > fabsf(b.x));
-                        const bool anyy = (ab.y > 0.0f) | (pc.y > 0.0f) | (s01.y > fabsf(a.y)) | (s23.y > fabsf(b.y));
-                        const bool allx = (dd[0].x > sd[0].x) & (dd[1].x > sd[1].x) & (dd[2].x > sd[2].x) &
-                                          (dd[3].x > sd[3].x);
-                        const bool ally = (dd[0].y > sd[0].y) & (dd[1].y > sd[1].y) & (dd[2].y > sd[2].y) &
-                                          (dd[3].y > sd[3].y);
-                        const float2 den = mul2(t0, bc(2.0f));
-                        if (condx & anyx & allx) ratio.x = dv(t2.x, den.x);
-                        if (condy & anyy & ally) ratio.y = dv(t2.y, den.y);
-                    }
-                    g[dir] = mul2(mul2(sums01, bc(0.5f)), sub2(bc(1.0f), ratio));
-                    const float2 e0 = sub2(dd[0], g[dir]), e1 = sub2(dd[1], g[dir]), e2 = sub2(dd[2], c),
-                                 e3 = sub2(dd[3], c);
-                    const float2 va = add2(make_float2(S.gvar[ty0 + oy[0]][tx0 + ox[0]], S.gvar[ty1 + oy[0]][tx1 + ox[0]]),
-                                           make_float2(S.gvar[ty0 + oy[1]][tx0 + ox[1]], S.gvar[ty1 + oy[1]][tx1 + ox[1]]));
-                    e[dir] = add2(dot4x2(e0, e1, e2, e3, e0, e1, e2, e3), va);
-                }
-                rbv = c;
-                const float2 num = mul2(sub2(g[0], g[1]), e[1]), den = add2(e[0], e[1]);
-                gv_out = add2(g[1], make_float2(dv(num.x, den.x), dv(num.y, den.y)));
-                const float2 vxx = variance2(rbv, d.chroma_off, nz);
-                S.vx[gy0][gx0] = vxx.x;
-                S.vx[gy1][gx1] = vxx.y;
-                S.sx[gy0][gx0] = rt(vxx.x);
-                S.sx[gy1][gx1] = rt(vxx.y);
-            }
-            const float2 vg = variance2(gv_out, d.chroma_off, nz);
-            S.rb[gy0][gx0] = rbv.x;
-            S.rb[gy1][gx1] = rbv.y;
-            S.gr[gy0][gx0] = gv_out.x;
-            S.gr[gy1][gx1] = gv_out.y;
-            S.sg[gy0][gx0] = rt(vg.x);
-            S.sg[gy1][gx1] = rt(vg.y);
-        }
-    } else
-    // Tiles at the picture edges: one site a thread, red/blue sites first
-    // (the heavy ones), 17 per region row, then green sites.
-    for (int k = tid; k < GH * (GW / 2) * 2; k += kDevThreads) {
-        const bool rbsite = k < GH * (GW / 2);
-        const int kk = rbsite ? k : k - GH * (GW / 2);
-        const int gy = kk / (GW / 2), j = kk - gy * (GW / 2);
+    // 2. Green pass on the region (the tile plus a 1-sensel halo).
+    // One site (gy, gx) of the region (src/demosaic.rs:481-541); the region
+    // row gy is picture row y0 - 1 + gy, the column gx picture column
+    // x0 - 1 + gx.
+    auto one_site = [&](int gy, int gx, bool rbsite) {
         const int y = y0 - 1 + gy;
         const bool phase = (y & 1) == red_row;
-        const int first = phase ? red_col : 1 - red_col;
-        // Region column gx maps to x = x0 - 1 + gx with x0 even.
-        const int gx = 2 * j + (rbsite ? 1 - first : first);
         const int x = x0 - 1 + gx;
-        if (y < 0 || y >= h || x < 0 || x >= w) continue;
+        if (y < 0 || y >= h || x < 0 || x >= w) return;
         const int ty = gy + 2, tx = gx + 2;  // nrm coordinates
         const float centre = S.nrm[ty][tx];
         float rbv = 0.0f, gv_out = centre;
@@ -669,6 +582,130 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
         S.rb[gy][gx] = rbv;
         S.gr[gy][gx] = gv_out;
         S.sg[gy][gx] = rt(variance(gv_out, d.chroma_off, nz));
+    };
+    // First green column mod 2 of region row gy (x0 and y0 are even).
+    auto first_of = [&](int gy) {
+        const bool phase = ((gy + 1) & 1) == red_row;
+        return phase ? red_col : 1 - red_col;
+    };
+    if (PRE && !near_edge) {
+        // Tiles clear of the edges: no mirror(), every site inside the
+        // picture. Two sites at a time as the lanes of pairs, lane x in
+        // region row gy0, lane y in row gy0 + 1 (the other colour).
+        auto site_pair = [&](bool rbsite, int gy0, int gx0, int gx1) {
+            const int gy1 = gy0 + 1;
+            const int ty0 = gy0 + 2, tx0 = gx0 + 2, ty1 = gy1 + 2, tx1 = gx1 + 2;  // nrm coordinates
+            const bool phase0 = ((gy0 + 1) & 1) == red_row;
+            const float2 clip = phase0 ? make_float2(d.clip[0], d.clip[1]) : make_float2(d.clip[1], d.clip[0]);
+            const float2 centre = make_float2(S.nrm[ty0][tx0], S.nrm[ty1][tx1]);
+            float2 rbv = make_float2(0.0f, 0.0f), gv_out = centre;
+            if (rbsite) {
+                const float2 c = make_float2(fminf(centre.x, clip.x), fminf(centre.y, clip.y));
+                const float2 sdc = make_float2(S.gsd[ty0][tx0], S.gsd[ty1][tx1]);
+                const bool condx = c.x > sdc.x, condy = c.y > sdc.y;
+                float2 g[2], e[2];
+    #pragma unroll
+                for (int dir = 0; dir < 2; dir++) {
+                    // Neighbours at distance 1 (green) and 2 (the centre's
+                    // colour), in the order of src/demosaic.rs:499-505.
+                    const int oy[4] = {dir ? -1 : 0, dir ? 1 : 0, dir ? -2 : 0, dir ? 2 : 0};
+                    const int ox[4] = {dir ? 0 : -1, dir ? 0 : 1, dir ? 0 : -2, dir ? 0 : 2};
+                    float2 dd[4], sd[4];
+    #pragma unroll
+                    for (int n = 0; n < 4; n++) {
+                        const float lx = n < 2 ? 1.0f : clip.x, ly = n < 2 ? 1.0f : clip.y;
+                        dd[n] = make_float2(fminf(S.nrm[ty0 + oy[n]][tx0 + ox[n]], lx),
+                                            fminf(S.nrm[ty1 + oy[n]][tx1 + ox[n]], ly));
+                        sd[n] = make_float2(S.gsd[ty0 + oy[n]][tx0 + ox[n]], S.gsd[ty1 + oy[n]][tx1 + ox[n]]);
+                    }
+                    const float2 sums01 = add2(dd[0], dd[1]), sums23 = add2(dd[2], dd[3]);
+                    float2 ratio = make_float2(0.0f, 0.0f);
+                    if (condx | condy) {
+                        const float2 t0 = add2(mul2(c, bc(2.0f)), sums23);
+                        const float2 t2 = add2(mul2(c, bc(-2.0f)), sums23);
+                        const float2 a = sub2(dd[0], dd[1]), b = sub2(dd[2], dd[3]);
+                        const float2 ab = mul2(a, b), pc = mul2(sub2(dd[2], c), sub2(dd[3], c));
+                        const float2 s01 = add2(sd[0], sd[1]), s23 = add2(sd[2], sd[3]);
+                        const bool anyx = (ab.x > 0.0f) | (pc.x > 0.0f) | (s01.x > fabsf(a.x)) | (s23.x > fabsf(b.x));
+                        const bool anyy = (ab.y > 0.0f) | (pc.y > 0.0f) | (s01.y > fabsf(a.y)) | (s23.y > fabsf(b.y));
+                        const bool allx = (dd[0].x > sd[0].x) & (dd[1].x > sd[1].x) & (dd[2].x > sd[2].x) &
+                                          (dd[3].x > sd[3].x);
+                        const bool ally = (dd[0].y > sd[0].y) & (dd[1].y > sd[1].y) & (dd[2].y > sd[2].y) &
+                                          (dd[3].y > sd[3].y);
+                        const float2 den = mul2(t0, bc(2.0f));
+                        if (condx & anyx & allx) ratio.x = dv(t2.x, den.x);
+                        if (condy & anyy & ally) ratio.y = dv(t2.y, den.y);
+                    }
+                    g[dir] = mul2(mul2(sums01, bc(0.5f)), sub2(bc(1.0f), ratio));
+                    const float2 e0 = sub2(dd[0], g[dir]), e1 = sub2(dd[1], g[dir]), e2 = sub2(dd[2], c),
+                                 e3 = sub2(dd[3], c);
+                    const float2 va = add2(make_float2(S.gvar[ty0 + oy[0]][tx0 + ox[0]], S.gvar[ty1 + oy[0]][tx1 + ox[0]]),
+                                           make_float2(S.gvar[ty0 + oy[1]][tx0 + ox[1]], S.gvar[ty1 + oy[1]][tx1 + ox[1]]));
+                    e[dir] = add2(dot4x2(e0, e1, e2, e3, e0, e1, e2, e3), va);
+                }
+                rbv = c;
+                const float2 num = mul2(sub2(g[0], g[1]), e[1]), den = add2(e[0], e[1]);
+                gv_out = add2(g[1], make_float2(dv(num.x, den.x), dv(num.y, den.y)));
+                const float2 vxx = variance2(rbv, d.chroma_off, nz);
+                S.vx[gy0][gx0] = vxx.x;
+                S.vx[gy1][gx1] = vxx.y;
+                S.sx[gy0][gx0] = rt(vxx.x);
+                S.sx[gy1][gx1] = rt(vxx.y);
+            }
+            const float2 vg = variance2(gv_out, d.chroma_off, nz);
+            S.rb[gy0][gx0] = rbv.x;
+            S.rb[gy1][gx1] = rbv.y;
+            S.gr[gy0][gx0] = gv_out.x;
+            S.gr[gy1][gx1] = gv_out.y;
+            S.sg[gy0][gx0] = rt(vg.x);
+            S.sg[gy1][gx1] = rt(vg.y);
+        };
+        // Each thread's quad of the tile (region rows 2 qy + 1, 2 qy + 2,
+        // columns 2 qx + 1, 2 qx + 2): its red/blue pair, the heavy work,
+        // one per thread.
+        {
+            const int gy0 = 2 * (tid >> 4) + 1, gxq = 2 * (tid & 15) + 1;
+            const int f0 = first_of(gy0);
+            site_pair(true, gy0, gxq + f0, gxq + 1 - f0);
+        }
+        // Then the 66 red/blue sites of the halo, one a thread, and the
+        // green sites as pairs (rows 2i and 2i + 1 of region quad (i, j)).
+        constexpr int kHalo = 2 * (GW / 2) + 2 * (TH / 2), kGreenPairs = (GH / 2) * (GW / 2);
+        const int g1 = first_of(1);
+        for (int u = tid; u < kHalo + kGreenPairs; u += kDevThreads) {
+            if (u < kHalo) {
+                int gy, gx;
+                if (u < GW / 2) {  // region row 0
+                    gy = 0;
+                    gx = 2 * u + 1 - first_of(0);
+                } else if (u < GW) {  // region row GH - 1
+                    gy = GH - 1;
+                    gx = 2 * (u - GW / 2) + 1 - first_of(GH - 1);
+                } else if (u < GW + TH / 2) {  // column 0: rows whose first green column is odd
+                    gy = 1 + 2 * (u - GW) + (g1 == 1 ? 0 : 1);
+                    gx = 0;
+                } else {  // column GW - 1: rows whose first green column is even
+                    gy = 1 + 2 * (u - GW - TH / 2) + (g1 == 0 ? 0 : 1);
+                    gx = GW - 1;
+                }
+                one_site(gy, gx, true);
+            } else {
+                const int uu = u - kHalo;
+                const int i = uu / (GW / 2), j = uu - i * (GW / 2);
+                const int f0 = first_of(2 * i);
+                site_pair(false, 2 * i, 2 * j + f0, 2 * j + 1 - f0);
+            }
+        }
+    } else {
+        // Tiles at the picture edges: one site a thread, red/blue sites
+        // first (the heavy ones), 17 per region row, then green sites.
+        for (int k = tid; k < GH * (GW / 2) * 2; k += kDevThreads) {
+            const bool rbsite = k < GH * (GW / 2);
+            const int kk = rbsite ? k : k - GH * (GW / 2);
+            const int gy = kk / (GW / 2), j = kk - gy * (GW / 2);
+            const int first = first_of(gy);
+            one_site(gy, 2 * j + (rbsite ? 1 - first : first), rbsite);
+        }
     }
     __syncthreads();
     // 3. Chroma (+ matrix) per quad.
