@@ -399,7 +399,8 @@ def run(args):
             line["e2e"] = {"value": e2e_value, "unit": "frames/s",
                            "h2d_bytes_per_step": int(np.mean([len(p) for p in pkts])),
                            "d2h_bytes_per_step": 12 * n + 16,
-                           "note": "prr_decode_develop_host from pinned host memory, 2 host threads, wall clock"}
+                           "note": f"prr_decode_develop_host from pinned host memory, {args.e2e_threads} host "
+                                   "threads, wall clock"}
         cl = clocks.summary()
         if cl:
             line["clocks"] = cl
@@ -413,8 +414,8 @@ def run(args):
 
 def measure_e2e(args, L, _lib, pkts, n, world):
     """Frames/s through prr_decode_develop_host: pinned host packet in,
-    pinned host planes out, with two contexts on two host threads so that
-    copies overlap kernels. Wall clock, max over ranks."""
+    pinned host planes out, with a context on each of --e2e-threads host
+    threads so that copies overlap kernels. Wall clock, max over ranks."""
     import torch
 
     host_pkts = []
@@ -422,7 +423,7 @@ def measure_e2e(args, L, _lib, pkts, n, world):
         hp = torch.empty(len(p), dtype=torch.uint8, pin_memory=True)
         hp.copy_(torch.frombuffer(bytearray(p), dtype=torch.uint8))
         host_pkts.append(hp)
-    nthreads = 2
+    nthreads = args.e2e_threads
     outs = [torch.empty(3 * n, dtype=torch.float32, pin_memory=True) for _ in range(nthreads)]
     ctxs = []
     for _ in range(nthreads):
@@ -559,6 +560,35 @@ def run_batch(args):
             dev_ms.append(dec.last_ms())
         wall = time.perf_counter() - t0
     launches = L.prr_kernel_launches() - launches0
+    # End to end: --batch-decoders decoders, each on a stream of its own,
+    # take turns, so that the next batches are parsed, staged and uploaded
+    # while batch k's kernels run (BatchDecoder.submit / wait).
+    bucket = dec.bucket(jobs)
+    nd = max(2, args.batch_decoders)
+    pipes = []
+    for _ in range(nd):
+        with torch.cuda.stream(torch.cuda.Stream()):
+            dk = P.BatchDecoder()
+        dk.set_config(bucket, cfg)
+        pipes.append((dk, [torch.empty_like(o) for o in outs]))
+
+    def pipelined(nsteps):
+        for st in range(min(nd - 1, nsteps)):
+            pipes[st][0].submit(jobs, pipes[st][1])
+        for st in range(nsteps):
+            if st + nd - 1 < nsteps:
+                dk, ok = pipes[(st + nd - 1) % nd]
+                dk.submit(jobs, ok)
+            res = pipes[st % nd][0].wait()
+            assert not any(isinstance(r, P.Error) for r in res)
+
+    pipelined(max(3, args.warmup))
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    pipelined(args.steps)
+    wall = time.perf_counter() - t0
     t = torch.tensor([sum(dev_ms), wall], dtype=torch.float64, device="cuda")
     if world > 1:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -584,8 +614,9 @@ def run_batch(args):
             "e2e": {"value": world * args.steps * nb / wall_max, "unit": "frames/s",
                     "h2d_bytes_per_step": sum(len(it.packet) for it in items),
                     "d2h_bytes_per_step": 16 * nb,
-                    "note": "BatchDecoder.decode from host packets: parse, upload, kernels, statuses back; "
-                            "frames stay on the device"},
+                    "note": "BatchDecoder.submit / wait from host packets (parse, stage, upload, kernels, "
+                            f"statuses back), {nd} decoders on streams of their own taking turns so that the next "
+                            "batches' uploads overlap a batch's kernels; frames stay on the device"},
         }
         cl = clocks.summary()
         if cl:
@@ -1381,6 +1412,10 @@ def main():
                     help="5k8 --overlap: cap the develop at this many CTAs per SM (0: as many as fit)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--batch-decoders", type=int, default=4,
+                    help="decoders taking turns in the mixed-batch end-to-end leg")
+    ap.add_argument("--e2e-threads", type=int, default=3,
+                    help="host threads (a context each) of the 5k8 end-to-end leg")
     args = ap.parse_args()
     if args.workload == "mixed-batch":
         return run_batch_reference(args) if args.impl == "reference" else run_batch(args)

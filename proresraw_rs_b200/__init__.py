@@ -638,7 +638,10 @@ class BatchDecoder:
     and the autotuner that picks them."""
 
     def __init__(self, device: Optional[int] = None):
+        # The context of the device's current stream: decoders made under
+        # different streams have contexts (and batch buffers) of their own.
         self.ctx = context(device)
+        self._pending = None
 
     def _prepare(self, jobs: Sequence[BatchJob], outs=None):
         torch = _torch()
@@ -702,11 +705,28 @@ class BatchDecoder:
     def decode(self, jobs: Sequence[BatchJob], outs=None) -> List[object]:
         """Decode every job; each result is a Frame, an RgbFrame or an Error.
         `outs` optionally gives each job's device output tensor."""
+        self.submit(jobs, outs)
+        return self.wait()
+
+    def submit(self, jobs: Sequence[BatchJob], outs=None) -> None:
+        """prr_batch_submit: parse and stage the batch, queue its upload and
+        kernels on the decoder's stream, and return without waiting for
+        them; wait() gives the results. One batch at a time per decoder (a
+        second submit before wait() raises PRR_ERR_INVALID). Two decoders
+        made under two streams pipeline: while one decoder's kernels run,
+        the other stages and uploads the next batch."""
         arr, keep, frames = self._prepare(jobs, outs)
-        L = _lib.lib()
-        _check(L.prr_batch_submit(self.ctx, arr, len(jobs)), ctx=self.ctx)
-        _check(L.prr_batch_wait(self.ctx, 0), ctx=self.ctx)
-        del keep
+        _check(_lib.lib().prr_batch_submit(self.ctx, arr, len(jobs)), ctx=self.ctx)
+        self._pending = (list(jobs), arr, keep, frames)
+
+    def wait(self, timeout_ms: int = 0) -> List[object]:
+        """prr_batch_wait: block until the submitted batch is decoded (0: no
+        time limit) and return its results, as decode() does."""
+        if self._pending is None:
+            raise _error(_lib.ERR_INVALID)
+        jobs, arr, keep, frames = self._pending
+        _check(_lib.lib().prr_batch_wait(self.ctx, timeout_ms), ctx=self.ctx)
+        self._pending = None
         return self._results(jobs, arr, frames)
 
     def last_ms(self) -> float:

@@ -142,3 +142,41 @@ def test_autotuner_picks_a_config_and_frames_stay_exact(corpus):
 def test_batch_of_one_large_frame_matches_single_decode():
     items = S.mixed_batch(2, seed=11, sizes=((1920, 1080),), corrupt=0.005)
     run_and_check(P.BatchDecoder(), jobs_of(items))
+
+
+def test_two_decoders_on_two_streams_pipeline(corpus):
+    # submit() returns with the batch queued; a second decoder, made under
+    # another stream, stages and submits the next batch before the first is
+    # waited for. Every batch still matches the oracle, outputs included
+    # after the other decoder has written its own.
+    import torch
+
+    jobs_a, jobs_b = jobs_of(corpus[:12]), jobs_of(corpus[12:])
+    decs = []
+    for _ in range(2):
+        with torch.cuda.stream(torch.cuda.Stream()):
+            decs.append(P.BatchDecoder())
+    assert decs[0].ctx.value != decs[1].ctx.value
+    want = {id(j): oracle_of(j) for j in jobs_a + jobs_b}
+    order = [jobs_a, jobs_b, jobs_a, jobs_b]
+    decs[0].submit(order[0])
+    for k in range(1, len(order) + 1):
+        if k < len(order):
+            decs[k % 2].submit(order[k])
+        got = decs[(k - 1) % 2].wait()
+        for job, g in zip(order[k - 1], got):
+            assert_job(job, g, want[id(job)])
+
+
+def test_submit_twice_or_wait_without_submit_is_invalid(corpus):
+    dec = P.BatchDecoder()
+    with pytest.raises(P.Error) as e:
+        dec.wait()
+    assert e.value.code == P._lib.ERR_INVALID
+    jobs = jobs_of(corpus[:4])
+    dec.submit(jobs)
+    with pytest.raises(P.Error) as e:
+        dec.submit(jobs)
+    assert e.value.code == P._lib.ERR_INVALID
+    for job, g in zip(jobs, dec.wait()):
+        assert_job(job, g, oracle_of(job))
