@@ -70,39 +70,49 @@ __device__ __forceinline__ void st_release(unsigned long long* p, unsigned long 
     asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-// Decoupled look-back (one thread): publish this tile's size, then sum the
+// Decoupled look-back by one warp: publish this tile's size, then sum the
 // sizes of the tiles before it back to the nearest published inclusive
-// prefix, and publish this tile's. Tiles are claimed in launch order, so
-// every tile before this one belongs to a CTA that is running or done; the
-// wait is bounded all the same. Returns the exclusive prefix, or ~0 if it
-// gave up.
-__device__ unsigned long long lookback(const Lj92Desc& d, uint32_t tile, unsigned long long slot) {
+// prefix, 32 tiles a step (lane l reads tile base - l), and publish this
+// tile's inclusive prefix. Tiles are claimed in launch order, so every tile
+// before this one belongs to a CTA that is running or done; the wait is
+// bounded all the same. Every lane returns the exclusive prefix, or ~0 if
+// the wait gave up.
+__device__ unsigned long long lookback_warp(const Lj92Desc& d, uint32_t tile, unsigned long long slot,
+                                            uint32_t lane) {
     if (tile == 0) {
-        st_release(d.lookback, kInclusive | slot);
+        if (lane == 0) st_release(d.lookback, kInclusive | slot);
         return 0;
     }
-    st_release(d.lookback + tile, kAggregate | slot);
+    if (lane == 0) st_release(d.lookback + tile, kAggregate | slot);
     unsigned long long excl = 0;
-    int64_t j = int64_t(tile) - 1;
+    int64_t base = int64_t(tile) - 1;
     uint32_t spins = 0;
-    while (j >= 0) {
-        const unsigned long long v = ld_acquire(d.lookback + j);
+    for (;;) {
+        const int64_t j = base - int64_t(lane);
+        // Before tile 0 there is nothing to add: an inclusive prefix of 0.
+        const unsigned long long v = j >= 0 ? ld_acquire(d.lookback + j) : kInclusive;
         const unsigned long long state = v & ~kValueMask;
-        if (state == 0) {
+        const uint32_t inc = __ballot_sync(0xFFFFFFFFu, state == kInclusive);
+        const uint32_t unpublished = __ballot_sync(0xFFFFFFFFu, state == 0);
+        // The lanes up to the nearest inclusive prefix (all 32 without one).
+        const uint32_t need = inc ? (inc ^ (inc - 1)) : 0xFFFFFFFFu;
+        if (unpublished & need) {
             if (++spins > kLookbackSpins) {
                 // Give up, and still publish, so that the tiles after this
                 // one do not wait too; the call reports the failure.
-                st_release(d.lookback + tile, kInclusive | slot);
+                if (lane == 0) st_release(d.lookback + tile, kInclusive | slot);
                 return ~0ull;
             }
             __nanosleep(64);
             continue;
         }
-        excl += v & kValueMask;
-        if (state == kInclusive) break;
-        j--;
+        unsigned long long part = ((need >> lane) & 1u) ? (v & kValueMask) : 0ull;
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xFFFFFFFFu, part, o);
+        excl += part;
+        if (inc) break;
+        base -= 32;
     }
-    st_release(d.lookback + tile, kInclusive | (excl + slot));
+    if (lane == 0) st_release(d.lookback + tile, kInclusive | (excl + slot));
     return excl;
 }
 
@@ -429,20 +439,22 @@ __global__ void __launch_bounds__(kLjThreads, 1) k_lj92_encode(Lj92Desc d) {
     carry = __shfl_sync(0xFFFFFFFFu, carry, 0);
     const uint64_t size = hdr + nbytes + total_ff + 2;
     const uint64_t slot = size + (d.pad_even ? (size & 1) : 0);
-    if (threadIdx.x == 0) {
-        d.sizes[tile_index] = uint32_t(size);
-        unsigned long long off = lookback(d, tile_index, slot);
-        if (off == ~0ull) {
-            atomicOr(d.error, 1u);
-        } else {
-            d.offsets[tile_index] = off;
-            if (tile_index == d.ntiles - 1) d.offsets[d.ntiles] = off + slot;
-            if (off + slot > d.out_cap) {
-                atomicOr(d.error, 2u);
-                off = ~0ull;
+    if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) d.sizes[tile_index] = uint32_t(size);
+        unsigned long long off = lookback_warp(d, tile_index, slot, threadIdx.x);
+        if (threadIdx.x == 0) {
+            if (off == ~0ull) {
+                atomicOr(d.error, 1u);
+            } else {
+                d.offsets[tile_index] = off;
+                if (tile_index == d.ntiles - 1) d.offsets[d.ntiles] = off + slot;
+                if (off + slot > d.out_cap) {
+                    atomicOr(d.error, 2u);
+                    off = ~0ull;
+                }
             }
+            s_offset = off;
         }
-        s_offset = off;
     }
     __syncthreads();
     if (s_offset == ~0ull) return;

@@ -215,6 +215,19 @@ def test_develop_edge_sizes(w, h):
         develop_compare(encoded(w, h, pattern=pattern, alignment=pattern % 5, seed=w * h + pattern))
 
 
+@pytest.mark.parametrize("pattern", range(4))
+def test_develop_when_paired_sites_take_different_branches(pattern):
+    # Interior tiles compute two sites as the two lanes of f32x2 pairs. A
+    # dark, noise-dominated mosaic (many estimates fall back to their mean)
+    # with clipped highlights makes the two sites of a pair take different
+    # branches often; neither lane's result may change.
+    m = S.mosaic(320, 200, pattern, seed=70 + pattern, sigma=40.0, specular=0.05, amp=(2.0, 60.0), white=4095)
+    spec = S.Spec(320, 200, pattern=pattern, alignment=2, white_level=4095, valid_tiles=True, wb=(2.4, 1.2))
+    pkt = S.encode(spec, m, qscale=(15, 45), qscale_seed=pattern)
+    develop_compare(pkt)
+    develop_compare(pkt, stages=(1, 2), wb=(0.6, 3.5))
+
+
 def test_encoded_frames_decode_and_develop_like_the_oracle():
     ident = [0, 8192, 16384, 24576, 32768, 40960, 49152, 57344]
     rng = np.random.default_rng(1)
