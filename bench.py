@@ -1430,8 +1430,9 @@ def main():
     ap.add_argument("--clip-batch", type=int, default=CLIP_BATCH, help="clip: frames per batch")
     ap.add_argument("--clip-threads", type=int, default=CLIP_THREADS, help="clip: reader threads")
     ap.add_argument("--dng-threads", type=int, default=4, help="dng: host threads of the end-to-end leg")
-    ap.add_argument("--overlap", action=argparse.BooleanOptionalAction, default=True,
-                    help="5k8: decode frame k+1 on a second, higher-priority stream while frame k develops")
+    ap.add_argument("--overlap", action=argparse.BooleanOptionalAction, default=None,
+                    help="5k8 / dng: decode frame k+1 on a second, higher-priority stream while frame k develops "
+                         "or is encoded (default: on for 5k8, off for dng, where it was measured slower)")
     ap.add_argument("--develop-ctas", type=int, default=0,
                     help="5k8 --overlap: cap the develop at this many CTAs per SM (0: as many as fit)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1441,6 +1442,8 @@ def main():
     ap.add_argument("--e2e-threads", type=int, default=3,
                     help="host threads (a context each) of the 5k8 end-to-end leg")
     args = ap.parse_args()
+    if args.overlap is None:
+        args.overlap = args.workload != "dng"
     if args.workload == "mixed-batch":
         return run_batch_reference(args) if args.impl == "reference" else run_batch(args)
     if args.workload == "clip":

@@ -131,84 +131,91 @@ struct HuffTable {
     uint8_t length[17];
 };
 
-// HuffmanTable::optimal (lj92.rs:96-202), by one thread.
-__device__ void build_table(const uint32_t* histogram, HuffTable& t) {
-    uint64_t freq[18];
-    for (int v = 0; v < 17; v++) freq[v] = histogram[v];
-    freq[17] = 1;  // the reserved symbol claims the all-ones code
-    int size[18], others[18];
-    for (int v = 0; v < 18; v++) size[v] = 0, others[v] = -1;
+// HuffmanTable::optimal (lj92.rs:96-202) by one warp: lane v holds symbol v
+// (categories 0-16, and 17, the reserved symbol of frequency 1). The two
+// least frequent trees come from two minimum reductions over a key that
+// orders by frequency, then by the larger symbol (the crate's tie rule); a
+// merge lengthens the codes of both trees' symbols (each lane carries the
+// symbol that holds its tree's frequency). The code-length limit, the value
+// order and the canonical codes follow with ballots and shuffles. A tile's
+// frequencies total at most 65536 + 1, so a key (frequency << 8 | 255 - v)
+// fits in 32 bits.
+__device__ void build_table(const uint32_t* histogram, HuffTable& t, uint32_t lane) {
+    constexpr uint32_t kAll = 0xFFFFFFFFu, kNone = 0xFFFFFFFFu;
+    uint32_t f = lane < 17 ? histogram[lane] : (lane == 17 ? 1u : 0u);
+    uint32_t label = lane, size = 0;
     for (;;) {
-        // The two least frequent symbols left; ties go to the larger symbol.
-        int least = -1, second = -1;
-        for (int v = 0; v < 18; v++) {
-            if (freq[v] == 0) continue;
-            if (least < 0 || freq[v] <= freq[least]) {
-                second = least;
-                least = v;
-            } else if (second < 0 || freq[v] <= freq[second]) {
-                second = v;
-            }
-        }
-        if (second < 0) break;
-        freq[least] += freq[second];
-        freq[second] = 0;
-        int v = least;
-        for (;;) {
-            size[v]++;
-            if (others[v] < 0) break;
-            v = others[v];
-        }
-        others[v] = second;
-        v = second;
-        for (;;) {
-            size[v]++;
-            if (others[v] < 0) break;
-            v = others[v];
-        }
+        const uint32_t key = f > 0 ? (f << 8) | (255u - lane) : kNone;
+        const uint32_t k1 = __reduce_min_sync(kAll, key);
+        const uint32_t v1 = 255u - (k1 & 255u);
+        const uint32_t k2 = __reduce_min_sync(kAll, lane == v1 ? kNone : key);
+        if (k2 == kNone) break;
+        const uint32_t v2 = 255u - (k2 & 255u);
+        if (lane == v1) f += k2 >> 8;
+        if (lane == v2) f = 0;
+        if (label == v1 || label == v2) size++;
+        if (label == v2) label = v1;
     }
-    uint32_t bits[33];
-    for (int i = 0; i < 33; i++) bits[i] = 0;
-    for (int v = 0; v < 18; v++)
-        if (size[v] > 0) bits[size[v]]++;
-    // Lengths limited to 16 (Figure K.3).
-    for (int i = 32; i > 16; i--) {
-        while (bits[i] > 0) {
-            int j = i - 2;
-            while (bits[j] == 0) j--;
-            bits[i] -= 2;
-            bits[i - 1] += 1;
-            bits[j + 1] += 2;
-            bits[j] -= 1;
-        }
+    // bits[i] in lane i: the symbols of code size i (at most 17 with 18
+    // symbols).
+    uint32_t bits = 0;
+    for (uint32_t i = 1; i < 32; i++) {
+        const uint32_t c = __popc(__ballot_sync(kAll, lane < 18 && size == i));
+        if (lane == i) bits = c;
     }
-    int i = 16;
-    while (bits[i] == 0) i--;
-    bits[i]--;  // the reserved symbol's code, the longest
+    // Lengths limited to 16 (Figure K.3); only size 17 can exceed it.
+    for (;;) {
+        if (__shfl_sync(kAll, bits, 17) == 0) break;
+        const uint32_t m = __ballot_sync(kAll, lane <= 15 && bits > 0);
+        if (m == 0) break;  // a code of 15 bits or less always exists
+        const uint32_t j = 31 - __clz(m);
+        if (lane == 17) bits -= 2;
+        if (lane == 16) bits += 1;
+        if (lane == j + 1) bits += 2;
+        if (lane == j) bits -= 1;
+    }
+    {
+        // The reserved symbol's code, the longest, is not used.
+        const uint32_t m = __ballot_sync(kAll, lane >= 1 && lane <= 16 && bits > 0);
+        if (m && lane == 31 - __clz(m)) bits -= 1;
+    }
     // HUFFVAL: used categories by (unlimited) code size, then value.
-    int n = 0;
-    for (int v = 0; v < 17; v++) {
-        if (size[v] == 0) continue;
-        int k = n++;
-        while (k > 0 && (size[t.values[k - 1]] > size[v])) {
-            t.values[k] = t.values[k - 1];
-            k--;
-        }
-        t.values[k] = uint8_t(v);
+    const bool used = lane < 17 && size > 0;
+    const uint32_t used_mask = __ballot_sync(kAll, used);
+    uint32_t rank = 0;
+    for (uint32_t u = 0; u < 17; u++) {
+        const uint32_t su = __shfl_sync(kAll, size, u);
+        if (((used_mask >> u) & 1u) && (su < size || (su == size && u < lane))) rank++;
     }
-    t.nvalues = uint32_t(n);
-    for (int k = 0; k < 16; k++) t.counts[k] = uint8_t(bits[k + 1]);
-    for (int v = 0; v < 17; v++) t.code[v] = 0, t.length[v] = 0;
-    uint32_t code = 0;
-    int k = 0;
-    for (int length = 1; length <= 16; length++) {
-        for (int c = 0; c < t.counts[length - 1]; c++) {
-            t.code[t.values[k]] = uint16_t(code);
-            t.length[t.values[k]] = uint8_t(length);
-            code++;
-            k++;
+    if (used) t.values[rank] = uint8_t(lane);
+    if (lane == 0) t.nvalues = uint32_t(__popc(used_mask));
+    const uint32_t cnt = (lane >= 1 && lane <= 16) ? bits : 0u;
+    if (lane >= 1 && lane <= 16) t.counts[lane - 1] = uint8_t(cnt);
+    // Canonical codes: the first code of length L is the sum over m < L of
+    // counts(m) << (L - m); a value's code is that plus its place among the
+    // values of its length.
+    uint32_t cum = cnt;  // inclusive scan of the counts over the lengths
+    for (uint32_t o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(kAll, cum, o);
+        if (lane >= o) cum += y;
+    }
+    uint32_t first = 0;
+    for (uint32_t m = 1; m < 16; m++) {
+        const uint32_t cm = __shfl_sync(kAll, cnt, m);
+        if (m < lane) first += cm << (lane - m);
+    }
+    uint32_t code = 0, length = 0;
+    for (uint32_t len = 1; len <= 16; len++) {
+        const uint32_t upto = __shfl_sync(kAll, cum, len), before = __shfl_sync(kAll, cum, len - 1);
+        const uint32_t start = __shfl_sync(kAll, first, len);
+        if (used && length == 0 && upto > rank) {
+            length = len;
+            code = start + (rank - before);
         }
-        code <<= 1;
+    }
+    if (lane < 17) {
+        t.code[lane] = uint16_t(code);
+        t.length[lane] = uint8_t(length);
     }
 }
 
@@ -351,15 +358,15 @@ __global__ void __launch_bounds__(kLjThreads, 1) k_lj92_encode(Lj92Desc d) {
     __syncthreads();
 
     // 2. The table.
-    if (threadIdx.x == 0) build_table(hist, table);
+    if (threadIdx.x < 32) build_table(hist, table, threadIdx.x);
     __syncthreads();
 
-    // 3. Bit offsets.
+    // 3. Bit offsets: this thread's bits from its category counts (each
+    // sample costs its category's code length, plus c extra bits for
+    // categories 1-15).
     uint64_t mine = 0;
-    for (uint32_t i = 0; i < run; i++) {
-        const uint32_t c = category(diffs[i * kLjPitch + col_t]);
-        mine += table.length[c] + ((c > 0 && c < 16) ? c : 0);
-    }
+#pragma unroll
+    for (int k = 0; k < 17; k++) mine += uint64_t(counts.get(k)) * (table.length[k] + ((k > 0 && k < 16) ? k : 0));
     uint64_t total_bits = 0;
     const uint64_t b0 = block_scan(mine, warp_sums, total_bits);
     uint32_t* words = d.words + uint64_t(tile_index) * d.word_cap;
@@ -409,6 +416,16 @@ __global__ void __launch_bounds__(kLjThreads, 1) k_lj92_encode(Lj92Desc d) {
         words[total_bits / 32] |= ((1u << pad) - 1) << (32 - used - pad);
     }
     __syncthreads();
+    // The differences are no longer needed: a stream that fits in their
+    // shared memory is copied there once (coalesced), and the two passes
+    // below read it from there instead of from L2.
+    const uint32_t* src = words;
+    if (nwords <= uint64_t(per) * kLjPitch / 2) {
+        uint32_t* staged = reinterpret_cast<uint32_t*>(diffs);
+        for (uint64_t w = threadIdx.x; w < nwords; w += kLjThreads) staged[w] = words[w];
+        src = staged;
+        __syncthreads();
+    }
 
     // 5. Byte stuffing: warp k takes words [k R, (k + 1) R) of the stream,
     // 32 at a time (a lane a word), counts their 0xFF bytes; the warps'
@@ -421,7 +438,7 @@ __global__ void __launch_bounds__(kLjThreads, 1) k_lj92_encode(Lj92Desc d) {
     const uint64_t R = (nwords + 31) / 32;
     const uint64_t wb = min(nwords, uint64_t(warp) * R), we = min(nwords, wb + R);
     auto word_ff = [&](uint64_t w, uint32_t& word, uint32_t& nb) -> uint32_t {
-        word = words[w];
+        word = src[w];
         const uint64_t left_bytes = nbytes - 4 * w;  // bytes of this word in the stream
         nb = left_bytes < 4 ? uint32_t(left_bytes) : 4u;
         uint32_t ff = 0;

@@ -138,3 +138,48 @@ def test_device_output_entry_point():
                              offs.data_ptr()) == _lib.ERR_BUFFER
     assert L.prr_lj92_encode(ctx, dimg.data_ptr(), 1, h, w, t, out.data_ptr(), cap,
                              offs.data_ptr()) == _lib.ERR_INVALID
+
+
+def image_of_differences(diffs, w, h):
+    # The image whose prediction differences, in coding order, are `diffs`
+    # (each sample less the one two to its left, the one above for a row's
+    # first two, 32768 for the first two of the first row; modulo 2^16).
+    img = np.zeros((h, w), dtype=np.int64)
+    k = 0
+    for r in range(h):
+        for c in range(w):
+            p = img[r, c - 2] if c >= 2 else (img[r - 1, c] if r > 0 else 32768)
+            img[r, c] = (p + int(diffs[k])) % 65536
+            k += 1
+    return img.astype(np.uint16).reshape(-1)
+
+
+def test_code_lengths_over_16_bits_are_limited_like_the_crate():
+    # Category counts 1, 2, 3, 5, 8, ... (Fibonacci) build a Huffman tree 17
+    # deep, so the table must go through the 16-bit length limit; the rest
+    # of the 128x128 tile goes to the largest category, which keeps the
+    # tree a chain.
+    rng = np.random.default_rng(17)
+    fib = [1, 2]
+    while len(fib) < 17:
+        fib.append(fib[-1] + fib[-2])
+    cats = rng.permutation(17)
+    counts = {int(cats[k]): fib[k] for k in range(17)}
+    big = int(cats[16])
+    counts[big] += 128 * 128 - sum(fib)
+    seq = np.concatenate([np.full(n, c) for c, n in counts.items()])
+    rng.shuffle(seq)
+    diffs = []
+    for c in seq:
+        if c == 0:
+            diffs.append(0)
+        elif c == 16:
+            diffs.append(32768)
+        else:
+            v = int(rng.integers(1 << (c - 1), 1 << c))
+            diffs.append(v if rng.random() < 0.5 else -v)
+    img = image_of_differences(diffs, 128, 128)
+    want = O.lj92_tiles(img, 128, 128, tile=128)
+    assert D.lj92_tiles(device(img, 128, 128), 128, 128, 128, 128) == want
+    samples, tw, th, c = decode(want[0])
+    assert samples == [int(v) for v in O.dng_tile(img, 128, 128, 0, 0, 128)]
