@@ -320,36 +320,70 @@ __global__ void __launch_bounds__(kLjThreads, 1) k_lj92_encode(Lj92Desc d) {
     const Geometry<TT> g(d.tile);
     const uint32_t T = g.T, n = T * T, per = g.per;
     if (threadIdx.x == 0) s_tile = atomicAdd(d.counter, 1u);
+    if (threadIdx.x < 17) hist[threadIdx.x] = 0;
     __syncthreads();
     const uint32_t tile_index = s_tile;
     const uint32_t left = tile_index % d.across * T, top = tile_index / d.across * T;
     const uint32_t s0 = min(n, threadIdx.x * per), s1 = min(n, s0 + per);
     const uint32_t run = s1 - s0;
     const uint32_t col_t = threadIdx.x;  // this thread's column of `diffs`
-    if (threadIdx.x < 17) hist[threadIdx.x] = 0;
 
-    // 0. The tile's differences, read row by row from the image (edges
-    // repeated as dng::tile does): each sample less the one two to its left
-    // (same Bayer colour), the one above for a row's first two, 32768 for
-    // the tile's first; modulo 2^16, centred on 0.
-    for (uint32_t s = threadIdx.x; s < n; s += kLjThreads) {
-        const uint32_t r = g.row(s), c = g.col(s);
-        const uint16_t* row = d.image + uint64_t(clamp_edge(top + r, d.height)) * d.stride;
-        const uint32_t x = __ldg(row + clamp_edge(left + c, d.width));
-        uint32_t p;
-        if (c >= 2)
-            p = __ldg(row + clamp_edge(left + c - 2, d.width));
-        else if (r > 0)
-            p = __ldg(d.image + uint64_t(clamp_edge(top + r - 1, d.height)) * d.stride + clamp_edge(left + c, d.width));
-        else
-            p = 32768u;
-        diffs[g.index(s)] = int16_t(uint16_t(x - p));
-    }
-    __syncthreads();
-
-    // 1. Categories.
+    // 0. The tile's differences (edges repeated as dng::tile does): each
+    // sample less the one two to its left (same Bayer colour), the one above
+    // for a row's first two, 32768 for the tile's first; modulo 2^16,
+    // centred on 0. 1. Each thread's counts of their categories, and the
+    // tile's histogram.
     Counts counts;
-    for (uint32_t i = 0; i < run; i++) counts.add(category(diffs[i * kLjPitch + col_t]));
+    const bool whole = TT == 256 && left + T <= d.width && top + T <= d.height &&
+                       (reinterpret_cast<uintptr_t>(d.image) & 15) == 0 && (d.stride & 7) == 0;
+    if (whole) {
+        // A 256-square tile inside the picture, rows 16-byte aligned: thread
+        // t loads its own run (row t / 4 of the tile, columns (t % 4) * 64
+        // on) with 16-byte loads and counts its categories as it goes.
+        const uint32_t r = threadIdx.x >> 2, c0 = (threadIdx.x & 3) * 64;
+        const uint16_t* row = d.image + uint64_t(top + r) * d.stride + left;
+        uint32_t p0 = 32768u, p1 = 32768u;  // the predictions of the next even and odd samples
+        if (c0 > 0 || r > 0) {
+            const uint32_t two = __ldg(reinterpret_cast<const uint32_t*>(c0 > 0 ? row + c0 - 2 : row - d.stride));
+            p0 = two & 0xFFFFu;
+            p1 = two >> 16;
+        }
+        const uint4* v = reinterpret_cast<const uint4*>(row + c0);
+#pragma unroll
+        for (uint32_t q = 0; q < 8; q++) {
+            const uint4 w = __ldg(v + q);
+            const uint32_t pairs[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (uint32_t h = 0; h < 4; h++) {
+                const uint32_t a = pairs[h] & 0xFFFFu, b = pairs[h] >> 16;
+                const int16_t da = int16_t(uint16_t(a - p0)), db = int16_t(uint16_t(b - p1));
+                const uint32_t i = 8 * q + 2 * h;
+                diffs[i * kLjPitch + col_t] = da;
+                diffs[(i + 1) * kLjPitch + col_t] = db;
+                counts.add(category(da));
+                counts.add(category(db));
+                p0 = a;
+                p1 = b;
+            }
+        }
+    } else {
+        // Any tile: coalesced loads in coding order, edges clamped.
+        for (uint32_t s = threadIdx.x; s < n; s += kLjThreads) {
+            const uint32_t r = g.row(s), c = g.col(s);
+            const uint16_t* row = d.image + uint64_t(clamp_edge(top + r, d.height)) * d.stride;
+            const uint32_t x = __ldg(row + clamp_edge(left + c, d.width));
+            uint32_t p;
+            if (c >= 2)
+                p = __ldg(row + clamp_edge(left + c - 2, d.width));
+            else if (r > 0)
+                p = __ldg(d.image + uint64_t(clamp_edge(top + r - 1, d.height)) * d.stride + clamp_edge(left + c, d.width));
+            else
+                p = 32768u;
+            diffs[g.index(s)] = int16_t(uint16_t(x - p));
+        }
+        __syncthreads();
+        for (uint32_t i = 0; i < run; i++) counts.add(category(diffs[i * kLjPitch + col_t]));
+    }
 #pragma unroll
     for (int k = 0; k < 17; k++) {
         const uint32_t sum = __reduce_add_sync(0xFFFFFFFFu, counts.get(k));
