@@ -6,22 +6,25 @@
 // JPEG image T/2 wide with two interleaved components, each sample
 // predicted from the one two columns to its left (same Bayer colour), the
 // one above for a row's first two, 32768 for the first. Passes:
-//   1. each thread takes a run of consecutive samples in coding order and
-//      counts their magnitude categories (warp sums, then 17 shared bins);
-//   2. one thread builds the tile's optimal Huffman table (Annex K.2 with a
+//   1. the tile's prediction differences go to shared memory; each thread
+//      takes a run of consecutive samples in coding order and counts their
+//      magnitude categories (warp sums, then 17 shared bins). In whole
+//      256-square tiles a thread loads its own run with 16-byte loads and
+//      counts as it goes; other tiles are read row by row, edges repeated;
+//   2. one warp builds the tile's optimal Huffman table (Annex K.2 with a
 //      reserved all-ones code, lengths limited to 16, canonical codes);
-//   3. each thread sums its samples' code + extra bits; a block scan gives
-//      every thread its bit offset in the tile's stream;
+//   3. each thread's bits follow from its category counts; a block scan
+//      gives every thread its bit offset in the tile's stream;
 //   4. each thread packs its bits, most significant first, into 32-bit
 //      words of a per-tile scratch stream (whole words stored, the shared
 //      first and last words OR-ed); the last byte is padded with ones;
-//   5. each warp takes a run of the stream's words, a lane a word at a
-//      time, and counts their 0xFF bytes; a scan places every byte, each
-//      0xFF followed by a stuffed 0x00; thread 0 writes the markers and
-//      the table around them.
-// A second kernel packs the tiles' streams back to back with their offsets.
-// The tile's samples are read from the image once, row by row, into shared
-// memory; the passes read them there.
+//   5. the stream is copied into the differences' shared memory when it
+//      fits; each warp takes a run of its words, a lane a word at a time,
+//      and counts their 0xFF bytes, which gives the stream's size;
+//   6. a warp's decoupled look-back over the tiles (claimed in launch
+//      order) gives the stream's offset in the output, and the CTA writes
+//      the markers, the table and the stream there, each 0xFF followed by
+//      a stuffed 0x00.
 
 #include <cuda_runtime.h>
 
