@@ -453,6 +453,14 @@ void prr_clip_destroy(prr_clip* clip);
 /* Begin decoding samples [first, first + count) at `scale` (PRR_SCALE_FULL
  * with `idct`, or a prr_scale with `greens`); ends any range in progress. */
 int prr_clip_start(prr_clip* clip, uint64_t first, uint64_t count, int scale, int idct, int greens);
+/* The range to decode after the current one, same arguments as
+ * prr_clip_start: once the current range's reads near their end, the
+ * pipeline reads and uploads the queued range's first batches, so that its
+ * first batch does not wait for its reads. prr_clip_next hands out the
+ * current range's end (n = 0), then the queued range's batches. One range
+ * queued at a time (PRR_ERR_INVALID for a second, or before any start);
+ * prr_clip_start drops a queued range. No counterpart in the crate. */
+int prr_clip_queue(prr_clip* clip, uint64_t first, uint64_t count, int scale, int idct, int greens);
 /* The next decoded batch, in order (n = 0 at the end). Its outputs stay valid
  * until the next call; work reading them must be enqueued on cuda_stream,
  * which orders it before the buffers are reused, or be complete by then.

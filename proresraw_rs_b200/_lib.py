@@ -299,6 +299,7 @@ def lib():
         "prr_clip_create_fd": (i, [i, i, P(CMovSample), sz, C.c_uint32, C.c_uint32, P(vp)]),
         "prr_clip_destroy": (None, [vp]),
         "prr_clip_start": (i, [vp, C.c_uint64, C.c_uint64, i, i, i]),
+        "prr_clip_queue": (i, [vp, C.c_uint64, C.c_uint64, i, i, i]),
         "prr_clip_next": (i, [vp, P(CClipBatch)]),
         "prr_clip_last_error": (C.c_char_p, [vp]),
         "prr_lj92_tile_bound": (C.c_uint64, [C.c_uint32]),

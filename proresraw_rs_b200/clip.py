@@ -67,6 +67,7 @@ class ClipDecoder:
                                                reader_threads, C.byref(h))
         _check(rc)
         self._h = h
+        self._ranges: list = []  # (scale, greens) of the current range, then the queued one
 
     @classmethod
     def from_fd(cls, fd: int, samples: Sequence[mov.Sample], frames_per_batch: int = 8,
@@ -83,7 +84,6 @@ class ClipDecoder:
                 idct: Idct = Idct.APPLE, greens: Greens = Greens.FIRST) -> Iterator[ClipBatch]:
         """Decode samples [first, first + count) (count None: to the end) at
         full resolution (scale None, with `idct`) or reduced."""
-        torch = _torch()
         L = _lib.lib()
         if count is None:
             count = self._n - first
@@ -91,6 +91,34 @@ class ClipDecoder:
         rc = L.prr_clip_start(self._h, first, count, sc, int(idct), int(greens))
         if rc != _lib.OK:
             raise RuntimeError(f"prr_clip_start: {rc} {self._last_error()}")
+        self._ranges = [(scale, greens)]
+        return self._iterate()
+
+    def queue(self, first: int = 0, count: Optional[int] = None, scale: Optional[Scale] = None,
+              idct: Idct = Idct.APPLE, greens: Greens = Greens.FIRST) -> None:
+        """prr_clip_queue: the range to decode after the current one; its
+        first batches are read and uploaded while the current range drains.
+        Iterate it with queued_batches() once the current range has ended."""
+        if count is None:
+            count = self._n - first
+        sc = _lib.SCALE_FULL if scale is None else int(scale)
+        rc = _lib.lib().prr_clip_queue(self._h, first, count, sc, int(idct), int(greens))
+        if rc != _lib.OK:
+            raise RuntimeError(f"prr_clip_queue: {rc} {self._last_error()}")
+        self._ranges.append((scale, greens))
+
+    def queued_batches(self) -> Iterator[ClipBatch]:
+        """The batches of the range queued with queue(), after the current
+        range's batches have all been taken."""
+        if len(getattr(self, "_ranges", [])) < 2:
+            raise RuntimeError("no range queued")
+        self._ranges.pop(0)
+        return self._iterate()
+
+    def _iterate(self) -> Iterator[ClipBatch]:
+        torch = _torch()
+        L = _lib.lib()
+        scale, greens = self._ranges[0]
         dev = torch.device("cuda", self.device)
         while True:
             b = _lib.CClipBatch()

@@ -59,6 +59,14 @@ struct ReadSlot {
     uint32_t claimed = 0, remaining = 0;  // under the clip's mutex
 };
 
+// A range of samples to decode: [first, first + count) in batches of the
+// clip's size, numbered from g0 in the clip's sequence of batches (a queued
+// range continues the numbering of the one before it).
+struct Range {
+    uint64_t first = 0, count = 0, nbatches = 0, g0 = 0;
+    int32_t scale = 0, idct = 0, greens = 0;
+};
+
 // A context (stream + batch state), its output buffer and the jobs of the
 // batch it holds.
 struct Lane {
@@ -87,13 +95,16 @@ struct prr_clip {
     bool stop = false;
     std::vector<std::thread> threads;
 
-    // The end of batch k's kernels, recorded on its lane when it is queued
-    // (slot k % 3 is recorded again only after batch k is finished): the
+    // The end of batch g's kernels, recorded on its lane when it is queued
+    // (slot g % 3 is recorded again only after batch g is finished): the
     // device time of a batch not overlapping the previous one.
     cudaEvent_t done[kReadSlots] = {};
-    uint64_t first = 0, count = 0, nbatches = 0, next_batch = 0;
-    int32_t scale = 0, idct = 0, greens = 0;
-    bool started = false;
+    // The current range, then the queued one (at most one). Batches are
+    // numbered across them: g_next is the next batch handed out; read slot
+    // g % 3 and lane g % 2 hold batch g.
+    std::deque<Range> ranges;
+    uint64_t g_next = 0;
+    bool ended = false;  // the current range's end (n = 0) has been handed out
     std::string last_error;
 
     int fail(int code, const std::string& m) {
@@ -127,25 +138,46 @@ struct prr_clip {
         }
     }
 
-    uint32_t batch_frames(uint64_t k) const {
-        return uint32_t(std::min<uint64_t>(per_batch, count - k * per_batch));
+    // The range holding batch g, and g's index in it (null past the ranges).
+    const Range* range_of(uint64_t g, uint64_t* k) const {
+        for (const Range& R : ranges)
+            if (g >= R.g0 && g < R.g0 + R.nbatches) {
+                *k = g - R.g0;
+                return &R;
+            }
+        return nullptr;
+    }
+    bool exists(uint64_t g) const {
+        uint64_t k;
+        return range_of(g, &k) != nullptr;
     }
 
-    // Bytes batch k's samples take in a read slot.
-    size_t slot_bytes(uint64_t k) const {
+    uint32_t batch_frames(const Range& R, uint64_t k) const {
+        return uint32_t(std::min<uint64_t>(per_batch, R.count - k * per_batch));
+    }
+
+    // Bytes batch k of range R takes in a read slot.
+    size_t slot_bytes(const Range& R, uint64_t k) const {
         size_t b = 0;
-        const uint64_t f0 = first + k * per_batch;
-        for (uint32_t i = 0; i < batch_frames(k); i++)
+        const uint64_t f0 = R.first + k * per_batch;
+        for (uint32_t i = 0; i < batch_frames(R, k); i++)
             b += up16(prr_padded_packet_bytes(size_t(samples[f0 + i].size)));
         return b;
     }
 
-    void schedule_read(uint64_t k) {
-        ReadSlot& r = slots[k % kReadSlots];
+    // Start the reads of batch g into read slot g % 3, whose previous batch
+    // (g - 3) has been handed out and uploaded: the slot grows here if a
+    // queued range has larger batches than the slots were sized for.
+    int schedule_read(uint64_t g) {
+        uint64_t k = 0;
+        const Range* R = range_of(g, &k);
+        if (!R) return fail(PRR_ERR_INVALID, "clip pipeline out of order");
+        ReadSlot& r = slots[g % kReadSlots];
+        PRR_TRY(cuda(r.buf.ensure(std::max<size_t>(slot_bytes(*R, k), 16))));
         std::lock_guard<std::mutex> lk(mu);
-        r.batch = k;
-        r.first = first + k * per_batch;
-        r.n = batch_frames(k);
+        r.batch = g;
+        r.first = R->first + k * per_batch;
+        r.n = batch_frames(*R, k);
         r.off.resize(r.n);
         r.status.assign(r.n, PRR_OK);
         r.message.assign(r.n, std::string());
@@ -157,8 +189,9 @@ struct prr_clip {
         r.bytes = o;
         r.claimed = 0;
         r.remaining = r.n;
-        work.push_back(int(k % kReadSlots));
+        work.push_back(int(g % kReadSlots));
         cv_work.notify_all();
+        return PRR_OK;
     }
 
     void wait_read(const ReadSlot& r) {
@@ -166,11 +199,16 @@ struct prr_clip {
         cv_done.wait(lk, [&] { return r.remaining == 0; });
     }
 
+    bool submitted(uint64_t g) const { return lanes[g % kLanes].pending && lanes[g % kLanes].batch == g; }
+
     // Upload and queue batch k on lane k % 2 once its samples are read.
     int submit(uint64_t k) {
+        uint64_t kr = 0;
+        const Range* R = range_of(k, &kr);
         Lane& L = lanes[k % kLanes];
         ReadSlot& r = slots[k % kReadSlots];
-        if (L.pending || r.batch != k) return fail(PRR_ERR_INVALID, "clip pipeline out of order");
+        if (!R || L.pending || r.batch != k) return fail(PRR_ERR_INVALID, "clip pipeline out of order");
+        const int32_t scale = R->scale, idct = R->idct, greens = R->greens;
         wait_read(r);
         L.jobs.assign(r.n, prr_job{});
         L.skipped.resize(r.n);
@@ -266,6 +304,29 @@ struct prr_clip {
     }
 };
 
+namespace {
+
+int check_range(const prr_clip* c, uint64_t first, uint64_t count, int scale) {
+    if (first > c->samples.size() || count > c->samples.size() - first) return PRR_ERR_INVALID;
+    if (scale != PRR_SCALE_FULL && (scale < 1 || scale > 3)) return PRR_ERR_INVALID;
+    return PRR_OK;
+}
+
+Range make_range(const prr_clip* c, uint64_t first, uint64_t count, int scale, int idct, int greens,
+                 uint64_t g0) {
+    Range R;
+    R.first = first;
+    R.count = count;
+    R.nbatches = (count + c->per_batch - 1) / c->per_batch;
+    R.g0 = g0;
+    R.scale = scale;
+    R.idct = idct;
+    R.greens = greens;
+    return R;
+}
+
+}  // namespace
+
 extern "C" {
 
 int prr_clip_create_fd(int device, int fd, const prr_mov_sample* samples, size_t n_samples,
@@ -328,45 +389,66 @@ void prr_clip_destroy(prr_clip* c) {
 
 int prr_clip_start(prr_clip* c, uint64_t first, uint64_t count, int scale, int idct, int greens) {
     if (!c) return PRR_ERR_INVALID;
-    if (first > c->samples.size() || count > c->samples.size() - first) return PRR_ERR_INVALID;
-    if (scale != PRR_SCALE_FULL && (scale < 1 || scale > 3)) return PRR_ERR_INVALID;
+    PRR_TRY(check_range(c, first, count, scale));
     if (cudaSetDevice(c->device) != cudaSuccess) return PRR_ERR_CUDA;
     c->drain();
-    c->first = first;
-    c->count = count;
-    c->nbatches = (count + c->per_batch - 1) / c->per_batch;
-    c->next_batch = 0;
-    c->scale = scale;
-    c->idct = idct;
-    c->greens = greens;
-    c->started = true;
+    c->ranges.clear();
+    c->ranges.push_back(make_range(c, first, count, scale, idct, greens, 0));
+    c->g_next = 0;
+    c->ended = false;
     for (ReadSlot& r : c->slots) r.batch = kNone;
     for (Lane& L : c->lanes) L.batch = kNone;
     // Every read slot sized for the largest batch of the range up front, so
     // that no pinned buffer is reallocated while batches are in flight.
+    const Range& R = c->ranges.front();
     size_t most = 0;
-    for (uint64_t k = 0; k < c->nbatches; k++) most = std::max(most, c->slot_bytes(k));
+    for (uint64_t k = 0; k < R.nbatches; k++) most = std::max(most, c->slot_bytes(R, k));
     for (ReadSlot& r : c->slots) PRR_TRY(c->cuda(r.buf.ensure(std::max<size_t>(most, 16))));
     return PRR_OK;
 }
 
+int prr_clip_queue(prr_clip* c, uint64_t first, uint64_t count, int scale, int idct, int greens) {
+    if (!c || c->ranges.empty()) return PRR_ERR_INVALID;
+    PRR_TRY(check_range(c, first, count, scale));
+    if (c->ended) {
+        // The current range is over (its n = 0 handed out): the queued one
+        // simply follows it.
+        c->ranges.pop_front();
+        c->ended = false;
+    } else if (c->ranges.size() > 1) {
+        return PRR_ERR_INVALID;  // one queued range at a time
+    }
+    const uint64_t g0 = c->ranges.empty() ? c->g_next : c->ranges.back().g0 + c->ranges.back().nbatches;
+    c->ranges.push_back(make_range(c, first, count, scale, idct, greens, g0));
+    return PRR_OK;
+}
+
 int prr_clip_next(prr_clip* c, prr_clip_batch* out) {
-    if (!c || !out || !c->started) return PRR_ERR_INVALID;
+    if (!c || !out || c->ranges.empty()) return PRR_ERR_INVALID;
     std::memset(out, 0, sizeof(*out));
     if (cudaSetDevice(c->device) != cudaSuccess) return PRR_ERR_CUDA;
-    const uint64_t k = c->next_batch;
-    if (k >= c->nbatches) return PRR_OK;  // the end of the range: n = 0
-    if (k == 0) {
-        c->schedule_read(0);
-        if (c->nbatches > 1) c->schedule_read(1);
-        PRR_TRY(c->submit(0));
+    const uint64_t g = c->g_next;
+    const Range& R = c->ranges.front();
+    if (g >= R.g0 + R.nbatches) {
+        // The end of the range: n = 0. A queued range becomes the current
+        // one; its first batches may already be read and queued.
+        if (c->ranges.size() > 1)
+            c->ranges.pop_front();
+        else
+            c->ended = true;
+        return PRR_OK;
     }
-    // The caller is done with batch k-1: its lane takes batch k+1, and its
-    // read slot (k+2's) takes the next reads.
-    if (k + 1 < c->nbatches) PRR_TRY(c->submit(k + 1));
-    if (k + 2 < c->nbatches) c->schedule_read(k + 2);
-    PRR_TRY(c->finish(k, out));
-    c->next_batch = k + 1;
+    // Batch g and g + 1 read, and g queued, unless an earlier call did so
+    // (a range's first batches, or a queued range's, read ahead).
+    if (c->slots[g % kReadSlots].batch != g) PRR_TRY(c->schedule_read(g));
+    if (c->exists(g + 1) && c->slots[(g + 1) % kReadSlots].batch != g + 1) PRR_TRY(c->schedule_read(g + 1));
+    if (!c->submitted(g)) PRR_TRY(c->submit(g));
+    // The caller is done with batch g - 1: its lane takes batch g + 1, and
+    // its read slot (g + 2's) takes the next reads, into a queued range too.
+    if (c->exists(g + 1) && !c->submitted(g + 1)) PRR_TRY(c->submit(g + 1));
+    if (c->exists(g + 2) && c->slots[(g + 2) % kReadSlots].batch != g + 2) PRR_TRY(c->schedule_read(g + 2));
+    PRR_TRY(c->finish(g, out));
+    c->g_next = g + 1;
     return PRR_OK;
 }
 

@@ -143,3 +143,51 @@ def test_a_callers_own_sample_table_and_descriptor(clip_path, packets):
             assert seen == 7
     finally:
         os.close(fd)
+
+
+def test_a_queued_range_follows_the_current_one(clip_path, packets):
+    # prr_clip_queue: the next range is read and uploaded while the current
+    # one drains, then handed out after the current range's end; a queued
+    # range may differ in scale and in batch bytes (a sub-range of the
+    # smaller frames first, the whole clip queued: the read slots grow).
+    small = [i for i, p in enumerate(packets) if len(p) < np.median([len(q) for q in packets])]
+    lo = small[0]
+    with mov.read_video_track(clip_path) as track, CL.ClipDecoder(track, 3, 2) as dec:
+        seen = []
+        for k, batch in enumerate(dec.batches(first=lo, count=2)):
+            if k == 0:
+                dec.queue(scale=P.Scale.HALF, greens=P.Greens.AVERAGE)
+            for i, got in enumerate(batch.frames):
+                assert_frame(got, oracle_of(packets[batch.first + i], None))
+            seen.append(batch.first)
+        assert seen == [lo]
+        n = 0
+        for batch in dec.queued_batches():
+            for i, got in enumerate(batch.frames):
+                assert_frame(got, oracle_of(packets[batch.first + i], P.Scale.HALF, greens=P.Greens.AVERAGE))
+            n += len(batch.frames)
+        assert n == len(packets)
+        # Queued after the current range has ended, and chained again.
+        dec.queue(first=4, count=5)
+        firsts = []
+        for k, batch in enumerate(dec.queued_batches()):
+            if k == 0:
+                dec.queue(first=0, count=3, idct=P.Idct.FFMPEG)
+            firsts.append(batch.first)
+            for i, got in enumerate(batch.frames):
+                assert_frame(got, oracle_of(packets[batch.first + i], None))
+        assert firsts == [4, 7]
+        for batch in dec.queued_batches():
+            for i, got in enumerate(batch.frames):
+                assert_frame(got, oracle_of(packets[batch.first + i], None, P.Idct.FFMPEG))
+        # An empty queued range; a second queued range is refused; a start
+        # drops a queued range.
+        it = dec.batches(first=0, count=4)
+        dec.queue(first=2, count=0)
+        with pytest.raises(RuntimeError):
+            dec.queue(first=0, count=1)
+        assert sum(len(b.frames) for b in it) == 4
+        assert list(dec.queued_batches()) == []
+        dec.batches(first=0, count=6)
+        dec.queue(first=6, count=6)
+        assert [b.first for b in dec.batches(first=9, count=4)] == [9, 12]

@@ -56,3 +56,11 @@ def test_the_library_refuses_to_run_without_a_device():
         pytest.skip("a device is present")
     with pytest.raises(RuntimeError):
         P.context()
+
+
+def test_clip_calls_refuse_a_null_pipeline():
+    # Host-side argument checks of the clip pipeline (no device touched).
+    L = _lib.lib()
+    assert L.prr_clip_start(None, 0, 1, _lib.SCALE_FULL, 0, 0) == _lib.ERR_INVALID
+    assert L.prr_clip_queue(None, 0, 1, _lib.SCALE_FULL, 0, 0) == _lib.ERR_INVALID
+    assert L.prr_clip_next(None, None) == _lib.ERR_INVALID
