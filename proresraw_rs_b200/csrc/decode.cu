@@ -837,13 +837,14 @@ __device__ __forceinline__ StreamJob stream_job(const FrameDesc& d, int greens, 
     return j;
 }
 
-// Entropy-decode the streams of tiles [chunk * blockDim.x / 4, ...) of a
-// frame, one stream per thread. `stage` holds stage_bytes + 16 bytes of
-// shared memory; the chunk's packet span is copied there when it fits.
-// Ends with the CTA's threads at different points (no barrier).
+// Entropy-decode the streams of tiles [chunk * 32, ...) of a frame, one
+// stream per thread of a 128-thread CTA. `stage` holds stage_bytes + 16
+// bytes of shared memory; the chunk's packet span is copied there when it
+// fits. `keys` holds 128 words of shared memory. Ends with the CTA's threads
+// at different points (no barrier).
 template <uint32_t LC>
 __device__ __forceinline__ void entropy_chunk(const EntropyTables& T, uint32_t* stage, uint32_t stage_bytes,
-                                              const FrameDesc& d, int greens,
+                                              uint32_t* keys, const FrameDesc& d, int greens,
                                               const uint32_t* __restrict__ tile_off, prr_dev_status* st,
                                               uint32_t chunk) {
     // The chunk's tiles [t0, t1) occupy bytes [tile_off[t0], tile_off[t1]).
@@ -861,8 +862,29 @@ __device__ __forceinline__ void entropy_chunk(const EntropyTables& T, uint32_t* 
             dst[i] = make_uint4(bswap32(v.x), bswap32(v.y), bswap32(v.z), bswap32(v.w));
         }
     }
+    // Threads take the chunk's streams in order of length (the shortest
+    // first), so that the streams of a warp end at about the same time: the
+    // kernel issues fewer warp instructions for the same symbols, which
+    // leaves more issue slots to the kernels beside it. Key: length << 7 |
+    // stream (128 streams a CTA), streams with nothing to decode last.
+    const StreamJob mine = stream_job<LC>(d, greens, tile_off, chunk * blockDim.x + threadIdx.x);
+    keys[threadIdx.x] = (mine.valid ? min(mine.slen, 0xFFFFFEu) : 0xFFFFFFu) << 7 | threadIdx.x;
     __syncthreads();
-    const StreamJob job = stream_job<LC>(d, greens, tile_off, chunk * blockDim.x + threadIdx.x);
+    for (uint32_t k = 2; k <= 128; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t i = threadIdx.x, l = i ^ j;
+            if (l > i) {
+                const uint32_t a = keys[i], b = keys[l];
+                if ((a > b) == ((i & k) == 0)) {
+                    keys[i] = b;
+                    keys[l] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const uint32_t pick = keys[threadIdx.x] & 127u;
+    const StreamJob job = pick == threadIdx.x ? mine : stream_job<LC>(d, greens, tile_off, chunk * blockDim.x + pick);
     if (!job.valid) return;
     uint32_t* list = d.pairs + stream_list_base(d, job.trow, job.x, job.log2, job.s, LC);
     bool revisited = false, ok = true;
@@ -879,10 +901,11 @@ __global__ void __launch_bounds__(128) k_entropy(FrameDesc d, int greens, const 
     __shared__ CodeTables CT;
     __shared__ EntropyTables T;
     __shared__ __align__(16) uint32_t stage[kStageBytes / 4 + 4];  // + the word after the last byte
+    __shared__ uint32_t keys[128];
     load_tables(&CT);
     __syncthreads();
     build_entropy_tables(T, CT);
-    entropy_chunk<LC>(T, stage, kStageBytes, d, greens, tile_off, st, blockIdx.x);
+    entropy_chunk<LC>(T, stage, kStageBytes, keys, d, greens, tile_off, st, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
