@@ -318,3 +318,36 @@ def test_develop_under_an_occupancy_cap_is_unchanged(ctas):
     finally:
         assert _lib.lib().prr_develop_set_occupancy(ctx, 0) == 0
     assert _lib.lib().prr_develop_set_occupancy(ctx, 17) == _lib.ERR_INVALID
+
+
+def test_a_c_program_decodes_and_develops_like_the_oracle(tmp_path):
+    # tests/c_abi/decode_develop.c: parse, params and prr_decode_develop_host
+    # from C, malloc'ed host buffers, no Python or torch in the process.
+    import os
+    import shutil
+    import subprocess
+
+    from proresraw_rs_b200 import _lib
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib_dir = os.path.dirname(_lib.LIB_PATH)
+    prog = str(tmp_path / "decode_develop")
+    subprocess.run([cc, "-std=c11", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "c_abi", "decode_develop.c"), "-o", prog, "-L", lib_dir, "-lprr",
+                    f"-Wl,-rpath,{lib_dir}"], check=True)
+    pkt = encoded(640, 352, pattern=3, alignment=4, qscale=45, sigma=24.0, specular=0.02, version=0, seed=77)
+    pkt, bad = S.corrupt_tiles(pkt, 0.05, seed=7)
+    (tmp_path / "frame.prr").write_bytes(pkt)
+    res = subprocess.run([prog, str(tmp_path / "frame.prr"), str(tmp_path / "planes.f32")], check=True,
+                         capture_output=True, text=True)
+    got = dict(line.split("=", 1) for line in res.stdout.splitlines())
+    o = O.decode_frame(pkt)
+    assert int(got["max_qscale"]) == o.max_qscale
+    assert [int(v) for v in got["skipped"].split(",") if v] == list(o.skipped_tiles)
+    want = O.develop(o, O.params_new(o.header, o.quantizer), 2, planar=True)
+    planes = np.fromfile(tmp_path / "planes.f32", dtype=np.float32).reshape(3, -1)
+    for c in range(3):
+        assert np.array_equal(planes[c].view(np.uint32), want[c].view(np.uint32)), c
