@@ -672,25 +672,29 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
         // green sites as pairs (rows 2i and 2i + 1 of region quad (i, j)).
         constexpr int kHalo = 2 * (GW / 2) + 2 * (TH / 2), kGreenPairs = (GH / 2) * (GW / 2);
         const int g1 = first_of(1);
-        for (int u = tid; u < kHalo + kGreenPairs; u += kDevThreads) {
-            if (u < kHalo) {
-                int gy, gx;
-                if (u < GW / 2) {  // region row 0
-                    gy = 0;
-                    gx = 2 * u + 1 - first_of(0);
-                } else if (u < GW) {  // region row GH - 1
-                    gy = GH - 1;
-                    gx = 2 * (u - GW / 2) + 1 - first_of(GH - 1);
-                } else if (u < GW + TH / 2) {  // column 0: rows whose first green column is odd
-                    gy = 1 + 2 * (u - GW) + (g1 == 1 ? 0 : 1);
-                    gx = 0;
-                } else {  // column GW - 1: rows whose first green column is even
-                    gy = 1 + 2 * (u - GW - TH / 2) + (g1 == 0 ? 0 : 1);
-                    gx = GW - 1;
-                }
-                one_site(gy, gx, true);
-            } else {
-                const int uu = u - kHalo;
+        // The halo's red/blue sites to the first kHalo threads, the (light)
+        // green pairs to the others, so that no thread takes a halo site and
+        // a green pair.
+        static_assert(kHalo < kDevThreads, "a halo site a thread");
+        if (tid < kHalo) {
+            const int u = tid;
+            int gy, gx;
+            if (u < GW / 2) {  // region row 0
+                gy = 0;
+                gx = 2 * u + 1 - first_of(0);
+            } else if (u < GW) {  // region row GH - 1
+                gy = GH - 1;
+                gx = 2 * (u - GW / 2) + 1 - first_of(GH - 1);
+            } else if (u < GW + TH / 2) {  // column 0: rows whose first green column is odd
+                gy = 1 + 2 * (u - GW) + (g1 == 1 ? 0 : 1);
+                gx = 0;
+            } else {  // column GW - 1: rows whose first green column is even
+                gy = 1 + 2 * (u - GW - TH / 2) + (g1 == 0 ? 0 : 1);
+                gx = GW - 1;
+            }
+            one_site(gy, gx, true);
+        } else {
+            for (int uu = tid - kHalo; uu < kGreenPairs; uu += kDevThreads - kHalo) {
                 const int i = uu / (GW / 2), j = uu - i * (GW / 2);
                 const int f0 = first_of(2 * i);
                 site_pair(false, 2 * i, 2 * j + f0, 2 * j + 1 - f0);
