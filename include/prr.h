@@ -535,7 +535,9 @@ int prr_dng_colour_of(const prr_header* header, prr_dng_colour* out);
 /* Value::srational / Value::rational (examples/prr2dng/tiff.rs:63-98). */
 int prr_dng_srational(double v, int32_t* num, int32_t* den);
 int prr_dng_rational(double v, uint32_t* num, uint32_t* den);
-/* quicktime_date_time (examples/prr2dng/dng.rs:226-246): UTC text of seconds since 1904. */
+/* quicktime_date_time (examples/prr2dng/dng.rs:226-246): UTC text of seconds
+ * since 1904, 19 characters and a NUL; PRR_ERR_BUFFER past the year 9999,
+ * whose text would be longer. */
 int prr_dng_date_time(uint64_t seconds, char out[20]);
 
 /* --- diagnostics -------------------------------------------------------------- */

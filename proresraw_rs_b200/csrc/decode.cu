@@ -27,14 +27,6 @@ namespace prr {
 
 namespace {
 
-__device__ __forceinline__ uint32_t warp_incl_scan_u32(uint32_t v, uint32_t lane) {
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t n = __shfl_up_sync(0xFFFFFFFFu, v, o);
-        if (lane >= uint32_t(o)) v += n;
-    }
-    return v;
-}
 __device__ __forceinline__ uint64_t warp_incl_scan_u64(uint64_t v, uint32_t lane) {
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {

@@ -478,9 +478,14 @@ int prr_dng_date_time(uint64_t seconds, char out[20]) {
     const int64_t day = doy - (153 * mp + 2) / 5 + 1;
     const int64_t month = mp < 10 ? mp + 3 : mp - 9;
     const int64_t year = yoe + era * 400 + (month <= 2 ? 1 : 0);
-    std::snprintf(out, 20, "%04lld:%02lld:%02lld %02llu:%02llu:%02llu", (long long)year, (long long)month,
-                  (long long)day, (unsigned long long)(time / 3600), (unsigned long long)(time / 60 % 60),
-                  (unsigned long long)(time % 60));
+    // The crate's text has 19 characters while the year has four digits;
+    // a later year does not fit the 20-byte result.
+    char text[64];
+    const int n = std::snprintf(text, sizeof(text), "%04lld:%02lld:%02lld %02llu:%02llu:%02llu", (long long)year,
+                                (long long)month, (long long)day, (unsigned long long)(time / 3600),
+                                (unsigned long long)(time / 60 % 60), (unsigned long long)(time % 60));
+    if (n != 19) return PRR_ERR_BUFFER;
+    std::memcpy(out, text, 20);
     return PRR_OK;
 }
 

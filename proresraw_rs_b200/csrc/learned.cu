@@ -82,8 +82,7 @@ constexpr size_t kParams = layer_off(kLayers);
 constexpr size_t kPacked = packed_off(kLayers);
 
 constexpr int TX = 32, TY = 16;          // output tile of a conv CTA
-constexpr int WX = TX + 2, WY = TY + 2;  // input window
-constexpr int kConvThreads = 256;  // two warpgroups; each reads back two of a tile's four M blocks
+constexpr int WY = TY + 2;              // input window rows
 constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
 
 // The window is staged as two overlapping halves of HX columns (window

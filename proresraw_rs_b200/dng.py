@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
-from . import FrameHeader, _check, _dptr, _lib, context
+from . import FrameHeader, _check, _dptr, _error, _lib, context
 
 
 class Samples(enum.IntEnum):
@@ -126,7 +126,9 @@ def rational(v: float) -> Tuple[int, int]:
 def quicktime_date_time(seconds: int) -> str:
     """dng.rs:226-246: UTC `YYYY:MM:DD HH:MM:SS` of a QuickTime time."""
     buf = C.create_string_buffer(20)
-    _lib.lib().prr_dng_date_time(int(seconds), buf)
+    rc = _lib.lib().prr_dng_date_time(int(seconds), buf)
+    if rc:
+        raise _error(rc)
     return buf.value.decode("ascii")
 
 

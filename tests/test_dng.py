@@ -122,6 +122,13 @@ def test_quicktime_dates():
     # 2021-10-23 12:34:56 UTC is Unix time 1634992496.
     assert D.quicktime_date_time(1_634_992_496 + 2_082_844_800) == "2021:10:23 12:34:56"
     assert D.quicktime_date_time(2_082_844_800 - 1) == "1969:12:31 23:59:59"
+    # The last second of the year 9999 still fits the 19 characters; the
+    # next one's text would be longer than the 20-byte result.
+    last = 253_402_300_799 + 2_082_844_800
+    assert D.quicktime_date_time(last) == "9999:12:31 23:59:59"
+    with pytest.raises(P.Error) as e:
+        D.quicktime_date_time(last + 1)
+    assert e.value.code == P._lib.ERR_BUFFER
 
 
 @pytest.mark.parametrize("cct,r,b", [(5235, 1.0, 1.0), (3200, 1.7, 0.6), (5139, 2.419, 1.5486)])
