@@ -75,17 +75,22 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def traffic_from_profiles(name: str = "develop_5760x3040.md"):
-    """DRAM bytes per launch of a kernel from its committed ncu summary
-    (a `traffic_bytes_per_launch:` line), if any."""
+def profile_value(name: str, key: str):
+    """A `key: number` line of a committed ncu summary under profiles/, if any."""
     path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1].strip())
     except OSError:
         pass
     return None
+
+
+def traffic_from_profiles(name: str = "develop_5760x3040.md"):
+    """DRAM bytes per launch of a kernel from its committed ncu summary
+    (a `traffic_bytes_per_launch:` line), if any."""
+    return profile_value(name, "traffic_bytes_per_launch")
 
 
 class Clocks:
@@ -405,6 +410,20 @@ def run(args):
         cl = clocks.summary()
         if cl:
             line["clocks"] = cl
+        # The develop kernel is bound by instruction issue, not by HBM: its
+        # warp instructions per launch (ncu smsp__inst_executed.sum, from the
+        # committed capture) over the same event-timed duration, against
+        # the SMs' issue rate at the sampled clock (4 schedulers an SM, one
+        # warp instruction a cycle each).
+        winst = profile_value("develop_5760x3040.md", "warp_instructions_per_launch")
+        mhz = (cl or {}).get("sm_mhz") or (cl or {}).get("sm_max_mhz")
+        if winst and mhz:
+            sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+            issue_peak = sms * 4 * mhz * 1e6
+            issue = winst / (dev_ms / 1000.0)
+            line["roofline"]["issue"] = {"warp_instructions_per_launch": winst, "achieved_per_s": issue,
+                                         "peak_per_s": issue_peak, "frac": issue / issue_peak,
+                                         "peak_source": f"{sms} SMs x 4 schedulers x {mhz} MHz"}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(pkts)
         print(json.dumps(line), flush=True)
