@@ -724,18 +724,20 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
             chroma_quad<0>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
         else
             chroma_quad<1>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
+        // The planes are written once and not read here again: streaming
+        // stores (evict first) leave L2 to the next frame's decode beside.
 #pragma unroll
         for (int dy = 0; dy < 2; dy++) {
             const size_t p = size_t(yb + dy) * w + xb;
             if (d.layout == PRR_PLANAR) {
-                *reinterpret_cast<float2*>(d.r + p) = o2[dy][0];
-                *reinterpret_cast<float2*>(d.g + p) = o2[dy][1];
-                *reinterpret_cast<float2*>(d.b + p) = o2[dy][2];
+                __stcs(reinterpret_cast<float2*>(d.r + p), o2[dy][0]);
+                __stcs(reinterpret_cast<float2*>(d.g + p), o2[dy][1]);
+                __stcs(reinterpret_cast<float2*>(d.b + p), o2[dy][2]);
             } else {
                 float2* o = reinterpret_cast<float2*>(d.r + 3 * p);
-                o[0] = make_float2(o2[dy][0].x, o2[dy][1].x);
-                o[1] = make_float2(o2[dy][2].x, o2[dy][0].y);
-                o[2] = make_float2(o2[dy][1].y, o2[dy][2].y);
+                __stcs(o, make_float2(o2[dy][0].x, o2[dy][1].x));
+                __stcs(o + 1, make_float2(o2[dy][2].x, o2[dy][0].y));
+                __stcs(o + 2, make_float2(o2[dy][1].y, o2[dy][2].y));
             }
         }
         return;
@@ -804,14 +806,14 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
     for (int dy = 0; dy < 2; dy++) {
         const size_t p = size_t(yb + dy) * w + xb;
         if (d.layout == PRR_PLANAR) {
-            *reinterpret_cast<float2*>(d.r + p) = make_float2(out[dy][0][0], out[dy][1][0]);
-            *reinterpret_cast<float2*>(d.g + p) = make_float2(out[dy][0][1], out[dy][1][1]);
-            *reinterpret_cast<float2*>(d.b + p) = make_float2(out[dy][0][2], out[dy][1][2]);
+            __stcs(reinterpret_cast<float2*>(d.r + p), make_float2(out[dy][0][0], out[dy][1][0]));
+            __stcs(reinterpret_cast<float2*>(d.g + p), make_float2(out[dy][0][1], out[dy][1][1]));
+            __stcs(reinterpret_cast<float2*>(d.b + p), make_float2(out[dy][0][2], out[dy][1][2]));
         } else {
             float2* o = reinterpret_cast<float2*>(d.r + 3 * p);
-            o[0] = make_float2(out[dy][0][0], out[dy][0][1]);
-            o[1] = make_float2(out[dy][0][2], out[dy][1][0]);
-            o[2] = make_float2(out[dy][1][1], out[dy][1][2]);
+            __stcs(o, make_float2(out[dy][0][0], out[dy][0][1]));
+            __stcs(o + 1, make_float2(out[dy][0][2], out[dy][1][0]));
+            __stcs(o + 2, make_float2(out[dy][1][1], out[dy][1][2]));
         }
     }
 }
