@@ -397,7 +397,14 @@ __device__ __forceinline__ void full_segment(SegShared& S, const FrameDesc& d, u
         const uint32_t r = t / vec_per_row, k = t - r * vec_per_row;
         const uint4 v = *reinterpret_cast<const uint4*>(stage + r * 256 + k * 8);
         uint16_t* dst = out + size_t(trow * 16 + r) * d.coded_w + seg * 256 + k * 8;
-        *reinterpret_cast<uint4*>(dst) = v;
+        // In the batch kernel the outputs are not read again soon: streaming
+        // stores (evict first) keep L2 for the coefficient lists the other
+        // segments read back. The single-frame decode keeps them cached for
+        // the develop that follows.
+        if (PERSIST)
+            __stcs(reinterpret_cast<uint4*>(dst), v);
+        else
+            *reinterpret_cast<uint4*>(dst) = v;
     }
 }
 
@@ -516,9 +523,15 @@ __device__ __forceinline__ void reduced_segment(SegShared& S, const FrameDesc& d
             rgb[2] = uint16_t(curve_apply(c0, cd, vals[(sq * 4 + 2) * 64 + at]));
         }
         uint16_t* dst = out + (size_t(trow * SIDE + i) * stride + seg * 16 * SIDE + px) * 3;
-        dst[0] = rgb[0];
-        dst[1] = rgb[1];
-        dst[2] = rgb[2];
+        if (PERSIST) {
+            __stcs(dst, rgb[0]);
+            __stcs(dst + 1, rgb[1]);
+            __stcs(dst + 2, rgb[2]);
+        } else {
+            dst[0] = rgb[0];
+            dst[1] = rgb[1];
+            dst[2] = rgb[2];
+        }
     }
 }
 
