@@ -441,10 +441,14 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(uint32_t(sizeof(box))), "r"(bar)
                      : "memory");
+        // The code values are read once here: an evict-first L2 policy on
+        // the load leaves L2 to the next frame's decode beside.
+        uint64_t policy;
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
         asm volatile(
-            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
-                "r"(smem_addr(&box[0][0])),
-            "l"(reinterpret_cast<uint64_t>(&codes_map)), "r"(bar), "r"(x0 - 8), "r"(y0 - 3)
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, "
+            "{%3, %4}], [%2], %5;" ::"r"(smem_addr(&box[0][0])),
+            "l"(reinterpret_cast<uint64_t>(&codes_map)), "r"(bar), "r"(x0 - 8), "r"(y0 - 3), "l"(policy)
             : "memory");
     }
     __syncthreads();
