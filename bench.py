@@ -35,6 +35,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -103,7 +104,9 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # The raw nvidia-smi samples (the line carries their summary).
+        out_dir = os.environ.get("PRR_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f"clocks_{os.getpid()}.csv")
         self.samples = []  # (sm_mhz, max_mhz, reasons)
         self._stop = threading.Event()
         self._thread = None
