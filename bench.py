@@ -48,6 +48,13 @@ from proresraw_rs_b200 import replicas as R  # noqa: E402
 
 W, H = 5760, 3040
 RING = 3
+# The workload of the default bench line, in both arms.
+WORKLOAD_5K8 = ("5760x3040 BGGR v0 align4 qscale45 qmat[4,63] 0.5% corrupt tiles; "
+                "decode_frame(Apple) + develop_planar_into(Rec2020)")
+CLIP_WORKLOAD = ("QuickTime clip of {nf} samples ({distinct} distinct 5760x3040 BGGR v0 align4 qscale45 packets, "
+                 "0.5% corrupt tiles), file in the page cache; decode_frame (Apple) of every sample")
+DNG_WORKLOAD = ("5760x3040 BGGR v0 align4 qscale45 qmat[4,63] 0.5% corrupt tiles; decode_frame (Apple) + "
+                "dng::write (code values, LinearizationTable, 256-square LJ92 tiles)")
 
 
 def make_packets(n: int):
@@ -94,41 +101,69 @@ def traffic_from_profiles(name: str = "develop_5760x3040.md"):
     return profile_value(name, "traffic_bytes_per_launch")
 
 
+def nvml_ids(dev: int):
+    """The NVML identities of CUDA device `dev`: its UUID and PCI bus id.
+    CUDA ordinals and NVML indices differ under a remapped
+    CUDA_VISIBLE_DEVICES, so the clock sampler never uses the ordinal."""
+    import torch
+
+    p = torch.cuda.get_device_properties(dev)
+    uuid = "GPU-" + str(p.uuid)
+    pci = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+    return uuid, pci
+
+
 class Clocks:
-    """SM clocks and clock-event reasons during the timed region: read through
-    NVML every 10 ms on a thread (short timed regions get samples too), with
-    `nvidia-smi -lms 200` beside it; reading only."""
+    """SM clocks and clock-event reasons, read through NVML every 10 ms on a
+    thread, with `nvidia-smi -lms 200` beside it; reading only. Samples carry
+    their time, so that the summary covers the settle phase (steps run for
+    at least a second right before the timed region, so that the clocks
+    reach their steady state under this load) and the timed region, and
+    counts the samples that fell inside the timed region itself."""
 
     NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index: int):
-        self.index = index
+    def __init__(self, dev: int):
+        self.uuid, self.pci = nvml_ids(dev)
         self.proc = None
         # The raw nvidia-smi samples (the line carries their summary).
         out_dir = os.environ.get("PRR_CLOCKS_DIR") or tempfile.gettempdir()
         self.path = os.path.join(out_dir, f"clocks_{os.getpid()}.csv")
-        self.samples = []  # (sm_mhz, max_mhz, reasons)
+        self.samples = []  # (time, sm_mhz, max_mhz, reasons)
         self._stop = threading.Event()
         self._thread = None
+        self.t_timed = None  # perf_counter at the start of the timed region
+        self.t_end = None
+
+    def _handle(self, N):
+        try:
+            return N.nvmlDeviceGetHandleByUUID(self.uuid.encode())
+        except Exception:
+            return N.nvmlDeviceGetHandleByPciBusId(self.pci.encode())
 
     def _nvml_loop(self):
         try:
             import pynvml as N
 
             N.nvmlInit()
-            h = N.nvmlDeviceGetHandleByIndex(self.index)
+            h = self._handle(N)
             bits = [N.nvmlClocksEventReasonHwSlowdown, N.nvmlClocksEventReasonHwThermalSlowdown,
                     N.nvmlClocksEventReasonSwThermalSlowdown, N.nvmlClocksEventReasonSwPowerCap]
             mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
             while True:
                 sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
                 r = N.nvmlDeviceGetCurrentClocksEventReasons(h)
-                self.samples.append((float(sm), float(mx), [n for n, b in zip(self.NAMES, bits) if r & b]))
+                self.samples.append((time.perf_counter(), float(sm), float(mx),
+                                     [n for n, b in zip(self.NAMES, bits) if r & b]))
                 if self._stop.wait(0.01):
                     break
             N.nvmlShutdown()
         except Exception:
             pass
+
+    def timed(self):
+        """Mark the start of the timed region."""
+        self.t_timed = time.perf_counter()
 
     def __enter__(self):
         self._thread = threading.Thread(target=self._nvml_loop, daemon=True)
@@ -137,7 +172,7 @@ class Clocks:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.index),
+                ["nvidia-smi", "-i", self.uuid,
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
@@ -148,6 +183,7 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        self.t_end = time.perf_counter()
         self._stop.set()
         if self._thread:
             self._thread.join(timeout=2)
@@ -161,10 +197,13 @@ class Clocks:
 
     def summary(self):
         sm, mx, reasons = [], [], set()
-        for s_mhz, m_mhz, rs in self.samples:
+        timed = 0
+        for t, s_mhz, m_mhz, rs in self.samples:
             sm.append(s_mhz)
             mx.append(m_mhz)
             reasons.update(rs)
+            if self.t_timed is not None and t >= self.t_timed:
+                timed += 1
         try:
             rows = [l.strip().split(", ") for l in open(self.path) if l.strip()]
         except OSError:
@@ -177,8 +216,27 @@ class Clocks:
             reasons.update(self.NAMES[i] for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active")
         if not sm:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        out = {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx) if mx else None,
+               "reasons": sorted(reasons), "samples": len(sm), "timed_region_nvml_samples": timed,
+               "window": "settle phase (>= 1 s of steps under the same load) + timed region", "nvml_device": self.uuid}
+        if self.t_timed is not None and self.t_end is not None:
+            out["settle_s"] = round(self.t_timed - (self.samples[0][0] if self.samples else self.t_timed), 3)
+        return out
+
+
+def settle(step_fn, min_s: float = 1.0, sync=None):
+    """Run steps for at least `min_s` of wall time (clocks reach their
+    steady state under the load) right before the timed region; returns
+    the number of steps run."""
+    k, t0 = 0, time.perf_counter()
+    while True:
+        step_fn(k)
+        k += 1
+        if k % 8 == 0 or k < 8:
+            if sync:
+                sync()
+            if time.perf_counter() - t0 >= min_s:
+                return k
 
 
 def cpu_baseline(pkts, budget_s: float = 15.0):
@@ -246,8 +304,7 @@ def run_reference(args):
         "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * el / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u16+f32", "data": "synthetic",
-        "config": {"workload": "5760x3040 BGGR v0 align4 qscale45 qmat[4,63] 0.5% corrupt tiles; "
-                               "decode_frame + develop_planar_into(Rec2020)", "frames_in_ring": RING},
+        "config": {"workload": WORKLOAD_5K8, "frames_in_ring": RING},
         "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} frames, CPU oracle (C++ restatement of the crate's rayon "
                                    f"path; the Rust crate cannot be built here), {threads} threads"},
@@ -349,11 +406,14 @@ def run(args):
 
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    launches0 = L.prr_kernel_launches()
     with Clocks(torch.cuda.current_device()) as clocks:
+        settle(step, 1.0, torch.cuda.synchronize)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        launches0 = L.prr_kernel_launches()
+        clocks.timed()
         start.record(s_dec)
         for k in range(args.steps):
             step(k, evs[k])
@@ -389,8 +449,7 @@ def run(args):
             "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u16+f32", "data": "synthetic",
-            "config": {"workload": "5760x3040 BGGR v0 align4 qscale45 qmat[4,63] 0.5% corrupt tiles; "
-                                   "decode_frame(Apple) + develop_planar_into(Rec2020)",
+            "config": {"workload": WORKLOAD_5K8,
                        "frames_in_ring": RING, "packet_bytes": [len(p) for p in pkts],
                        "l2": "inputs+outputs > L2 (210 MB planes written per step)",
                        "parallelism": f"replicas x{world}",
@@ -571,12 +630,14 @@ def run_batch(args):
         cfg, tuned_ms = dec.tune(jobs, reps=2)
     for _ in range(max(3, args.warmup)):
         dec.decode(jobs, outs)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    launches0 = L.prr_kernel_launches()
     dev_ms = []
     with Clocks(torch.cuda.current_device()) as clocks:
+        settle(lambda k: dec.decode(jobs, outs), 1.0)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        launches0 = L.prr_kernel_launches()
+        clocks.timed()
         t0 = time.perf_counter()
         for _ in range(args.steps):
             dec.decode(jobs, outs)
@@ -756,11 +817,13 @@ def run_clip(args):
 
         assert passes(2, check=True)[0] == 2 * nf
         passes(max(3, args.warmup))
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-        launches0 = L.prr_kernel_launches()
         with Clocks(torch.cuda.current_device()) as clocks:
+            settle(lambda k: passes(1), 1.0, torch.cuda.synchronize)
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            launches0 = L.prr_kernel_launches()
+            clocks.timed()
             t0 = time.perf_counter()
             dev_total = passes(args.steps)[1]
             torch.cuda.synchronize()
@@ -802,9 +865,7 @@ def run_clip(args):
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-                "config": {"workload": f"QuickTime clip of {nf} samples ({CLIP_DISTINCT} distinct {W}x{H} BGGR v0 "
-                                       "align4 qscale45 packets, 0.5% corrupt tiles), file in the page cache; "
-                                       "decode_frame (Apple) of every sample",
+                "config": {"workload": CLIP_WORKLOAD.format(nf=nf, distinct=CLIP_DISTINCT),
                            "frames_per_step": nf, "frames_per_batch": args.clip_batch,
                            "reader_threads": args.clip_threads, "clip_bytes": os.path.getsize(path),
                            "l2": f"{2 * cw * ch * nf / 1e9:.1f} GB of code values written per pass, more than L2",
@@ -853,7 +914,7 @@ def run_clip_reference(args):
         "impl": "reference", "metric": CLIP_METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / n * args.clip_frames,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": {"workload": f"QuickTime clip of {args.clip_frames} {W}x{H} samples; read_at + decode_frame",
+        "config": {"workload": CLIP_WORKLOAD.format(nf=args.clip_frames, distinct=CLIP_DISTINCT),
                    "frames_per_step": args.clip_frames},
         "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
                          "sample": f"{n} samples read and decoded by the CPU oracle, {threads} threads, {el:.1f} s"},
@@ -958,11 +1019,14 @@ def run_dng(args):
     tile_bytes = int(offsets[-1].item())
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    launches0 = L.prr_kernel_launches()
     with Clocks(torch.cuda.current_device()) as clocks:
+        settle(step, 1.0, torch.cuda.synchronize)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        launches0 = L.prr_kernel_launches()
+        clocks.timed()
         start.record(s_dec)
         for k in range(args.steps):
             step(k, evs[k])
@@ -1050,8 +1114,7 @@ def run_dng(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
             "data": "synthetic",
-            "config": {"workload": f"{W}x{H} BGGR v0 align4 qscale45 qmat[4,63] 0.5% corrupt tiles; decode_frame "
-                                   "(Apple) + dng::write (code values, LinearizationTable, 256-square LJ92 tiles)",
+            "config": {"workload": DNG_WORKLOAD,
                        "frames_in_ring": RING, "tiles_per_frame": ntiles, "tile_bytes_per_frame": tile_bytes,
                        "dng_file_bytes": file_bytes[-1] if file_bytes else None,
                        "l2": "35 MB of code values and about 20 MB of streams a frame; 3 distinct frames (not "
@@ -1095,7 +1158,7 @@ def run_dng_reference(args):
         "impl": "reference", "metric": DNG_METRIC, "value": v, "unit": "frames/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / n, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": {"workload": f"{W}x{H} frames; decode_frame + LJ92 tiles of dng::write"},
+        "config": {"workload": DNG_WORKLOAD},
         "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
                          "sample": f"{n} frames, CPU oracle decode + LJ92 tiles, {threads} threads, {el:.1f} s"},
         "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -1199,8 +1262,11 @@ def run_learned(args):
         f = frames[k % len(frames)]
         P.develop_planar_into(f, prms[k % len(frames)], P.Stage.REC2020, out)
 
-    launches0 = P.kernel_launches()
     with Clocks(torch.cuda.current_device()) as clocks:
+        settle(learned_step, 1.0, torch.cuda.synchronize)
+        torch.cuda.synchronize()
+        launches0 = P.kernel_launches()
+        clocks.timed()
         ms_learned = timed(learned_step, args.steps)
     launches = P.kernel_launches() - launches0
     ms_plain = timed(plain_step, args.steps)
@@ -1400,11 +1466,14 @@ def run_stream(args):
 
     run_steps(max(3, args.warmup))
     torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = P.kernel_launches()
     with Clocks(torch.cuda.current_device()) as clocks:
+        settle(lambda k: run_steps(1), 1.0, torch.cuda.synchronize)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        launches0 = P.kernel_launches()
+        clocks.timed()
         t0 = time.perf_counter()
         e0.record(side)
         dec_ms = run_steps(args.steps)
@@ -1470,17 +1539,184 @@ def run_stream(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Linearize workload: Frame::linearize_into of decoded 5760x3040 frames
+# (code values through the frame's 8-point curve, src/curve.rs:14-33,
+# src/decoder.rs:197-216), device-resident; a ring of LIN_RING frames of
+# code values and outputs (4 x 70 MB, more than L2). One step = one frame.
+LIN_RING = 4
+LIN_WORKLOAD = ("5760x3040 BGGR v0 align4 qscale45 frames (decoded code values, curve of the header); "
+                "Frame::linearize_into")
+
+
+def run_linearize(args):
+    import torch
+
+    import proresraw_rs_b200 as P
+    from proresraw_rs_b200 import _lib
+
+    world, rank, local = dist_setup(args.gpus)
+    L = _lib.lib()
+    pkts = make_packets(RING)
+    frames = [P.decode_frame(pkts[k % RING]) for k in range(LIN_RING)]
+    n = W * H
+    outs = [torch.empty(n, dtype=torch.uint16, device="cuda") for _ in range(LIN_RING)]
+    s = torch.cuda.Stream()
+    ctx = C.c_void_p()
+    assert L.prr_ctx_create(torch.cuda.current_device(), C.c_void_p(s.cuda_stream), C.byref(ctx)) == 0
+    torch.cuda.synchronize()
+
+    def step(k, ev=None):
+        f, o = frames[k % LIN_RING], outs[k % LIN_RING]
+        if ev:
+            ev[0].record(s)
+        assert L.prr_linearize(ctx, C.byref(f.header._c), f.samples.data_ptr(), o.data_ptr(), n) == 0
+        if ev:
+            ev[1].record(s)
+
+    for k in range(max(3, args.warmup)):
+        step(k)
+    torch.cuda.synchronize()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+
+    want = O.decode_frame(pkts[0], 0, os.cpu_count() or 1).linearize(os.cpu_count() or 1)
+    assert np.array_equal(outs[0].cpu().numpy().view(np.uint16), want.reshape(-1)), "linearize differs"
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(torch.cuda.current_device()) as clocks:
+        settle(step, 1.0, torch.cuda.synchronize)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        launches0 = L.prr_kernel_launches()
+        clocks.timed()
+        start.record(s)
+        for k in range(args.steps):
+            step(k, evs[k])
+        end.record(s)
+        torch.cuda.synchronize()
+    launches = L.prr_kernel_launches() - launches0
+    ms = R.reduce_max(start.elapsed_time(end))
+    lin_ms = sum(e[0].elapsed_time(e[1]) for e in evs) / args.steps
+    value = world * args.steps / (ms / 1000.0)
+    # End to end: host code values in (pinned), linear values out (pinned).
+    e2e = None
+    if not args.no_e2e:
+        hin = torch.empty(n, dtype=torch.uint16, pin_memory=True)
+        hin.copy_(frames[0].samples.cpu())
+        hout = torch.empty(n, dtype=torch.uint16, pin_memory=True)
+        din, dout = torch.empty(n, dtype=torch.uint16, device="cuda"), outs[0]
+        hdr = frames[0].header._c
+
+        def e2e_step():
+            with torch.cuda.stream(s):
+                din.copy_(hin, non_blocking=True)
+                assert L.prr_linearize(ctx, C.byref(hdr), din.data_ptr(), dout.data_ptr(), n) == 0
+                hout.copy_(dout, non_blocking=True)
+
+        for _ in range(3):
+            e2e_step()
+        s.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        s.synchronize()
+        e2e = R.reduce_max(time.perf_counter() - t0)
+        e2e = world * args.steps / e2e
+    L.prr_ctx_destroy(ctx)
+    if rank == 0:
+        peak, peak_kind = peaks()
+        alg = 4 * n
+        achieved = alg / (lin_ms / 1000.0) / 1e9
+        line = {
+            "metric": "5.8K frames/s linearize", "value": value, "unit": "frames/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "config": {"workload": LIN_WORKLOAD, "frames_in_ring": LIN_RING,
+                       "l2": "inputs+outputs > L2 (4 x 70 MB ring)", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": "k_linearize", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profile_value("linearize_5760x3040.md",
+                                                                           "traffic_bytes_per_launch"),
+                         "peak_source": f"{peak_kind} hbm_gbs", "algorithmic_bytes_per_launch": alg,
+                         "kernel_ms": lin_ms},
+            "gpu_launches": int(launches),
+        }
+        if e2e is not None:
+            line["e2e"] = {"value": e2e, "unit": "frames/s", "h2d_bytes_per_step": 2 * n, "d2h_bytes_per_step": 2 * n,
+                           "note": "pinned host code values in, linear values out, one stream, wall clock"}
+        cl = clocks.summary()
+        if cl:
+            line["clocks"] = cl
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = linearize_cpu(pkts[0], 10.0)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def linearize_cpu(pkt, budget_s: float):
+    """The oracle's Frame::linearize on the host cores, frames/s over a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+
+    threads = os.cpu_count() or 1
+    f = O.decode_frame(pkt, 0, threads)
+    f.linearize(threads)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        f.linearize(threads)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or n >= 2000:
+            break
+    return {"value": n / el, "unit": "frames/s", "cores": threads, "kind": "port",
+            "sample": f"{n} linearizations of a {W}x{H} frame, CPU oracle, {threads} threads, {el:.1f} s"}
+
+
+def run_linearize_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle as O
+
+    threads = os.cpu_count() or 1
+    f = O.decode_frame(make_packets(1)[0], 0, threads)
+    for _ in range(args.warmup):
+        f.linearize(threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        f.linearize(threads)
+    el = time.perf_counter() - t0
+    v = args.steps / el
+    line = {
+        "impl": "reference", "metric": "5.8K frames/s linearize", "value": v, "unit": "frames/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": LIN_WORKLOAD, "frames_in_ring": LIN_RING},
+        "cpu_baseline": {"value": v, "unit": "frames/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} linearizations, CPU oracle, {threads} threads"},
+        "e2e": {"value": v, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="5k8", choices=["5k8", "mixed-batch", "learned", "8k-stream", "clip", "dng"],
+    ap.add_argument("--workload", default="5k8", choices=["5k8", "mixed-batch", "learned", "8k-stream", "clip", "dng",
+                                                               "linearize"],
                     help="5k8: the headline single-frame decode+develop; mixed-batch: 64 uneven frames per step; "
                          "learned: surrogate develop of 4K frames (trains first); 8k-stream: 16 8K frames per step; "
                          "clip: a movie file of 5.8K frames through the clip pipeline, one pass per step; "
-                         "dng: 5.8K frames decoded and exported as DNG files (LJ92 tiles on the device)")
+                         "dng: 5.8K frames decoded and exported as DNG files (LJ92 tiles on the device); "
+                         "linearize: Frame::linearize_into of decoded 5.8K frames")
     ap.add_argument("--epochs", type=int, default=8, help="training epochs for the learned workloads")
     ap.add_argument("--save-model", default="", help="learned: save the trained surrogate (.npz)")
     ap.add_argument("--model", default=os.path.join(ROOT, "proresraw_rs_b200", "data", "surrogate.npz"),
@@ -1511,6 +1747,8 @@ def main():
         return run_clip_reference(args) if args.impl == "reference" else run_clip(args)
     if args.workload == "dng":
         return run_dng_reference(args) if args.impl == "reference" else run_dng(args)
+    if args.workload == "linearize":
+        return run_linearize_reference(args) if args.impl == "reference" else run_linearize(args)
     if args.workload in ("learned", "8k-stream"):
         if args.impl == "reference":
             return run_reference(args)

@@ -212,9 +212,12 @@ int prr_decode_reduced_async(prr_ctx* ctx, const prr_frame_info* info, const uin
  * that loads the library until the process exits. Frames with more tiles
  * return PRR_ERR_SCRATCH_LIMIT. The first call on a device looks the array
  * up (with `device` made current) and should come before any stream
- * capture on that device. All calls share the array: calls whose work
- * overlaps on the GPU (other streams, other threads) race; serialize them
- * on one stream. `cuda_stream` is a cudaStream_t (NULL: legacy default). */
+ * capture on that device; the address is kept for the life of the process
+ * and is not valid after a cudaDeviceReset. All calls share the array:
+ * calls whose work overlaps on the GPU (other streams, other threads) race;
+ * serialize them on one stream. `cuda_stream` is a cudaStream_t (NULL:
+ * legacy default). `device` is an ordinal below 64 (else PRR_ERR_INVALID);
+ * the calling thread's current device is the same on return as on entry. */
 int prr_decode_noalloc(int device, void* cuda_stream, const prr_frame_info* info,
                        const uint8_t* dev_packet, int idct, uint16_t* dev_samples,
                        prr_dev_status* dev_status, uint32_t* dev_skipped);
@@ -274,6 +277,19 @@ int prr_batch_tune(prr_ctx* ctx, prr_job* jobs, size_t n, uint32_t reps, prr_bat
                    float* best_ms);
 /* Set or read the config of a bucket (unset buckets use the default). */
 int prr_batch_set_config(prr_ctx* ctx, uint32_t bucket, const prr_batch_config* cfg);
+/* The batch kernel's transform segments wait for the entropy chunks of
+ * their tiles through flags in device memory; each wait gives up after
+ * this many microseconds (0: the default of 2 s), the segment is left
+ * unwritten and its frame's job reports PRR_ERR_TIMEOUT while the other
+ * frames of the batch and the context stay usable. Applies to the batches
+ * submitted after the call. No counterpart in the crate: its one device
+ * wait is the map of a download buffer (src/gpu.rs:1231-1278). */
+int prr_batch_set_wait_limit(prr_ctx* ctx, uint32_t microseconds);
+/* Test hook for that limit: from the next batch on, entropy chunk `chunk`
+ * (counted over the batch's frames in job order, 128 tiles a chunk) is
+ * claimed and abandoned, as a CTA that died would leave it, so its flag is
+ * never set. 0xFFFFFFFF turns it off. */
+int prr_batch_drop_chunk_for_test(prr_ctx* ctx, uint32_t chunk);
 int prr_batch_get_config(prr_ctx* ctx, uint32_t bucket, prr_batch_config* cfg);
 
 /* --- linearize ---------------------------------------------------------------- */
@@ -472,7 +488,7 @@ const char* prr_clip_last_error(const prr_clip* clip);
 /* --- DNG export (examples/prr2dng) --------------------------------------------- */
 /* Lossless JPEG tiles of a 16-bit CFA image (DNG compression 7): the tile x
  * tile squares of the image, row by row, each cut as dng::tile does
- * (examples/prr2dng/dng.rs:114-125: sensels past the right or bottom edge
+ * (examples/prr2dng/dng.rs:115-127: sensels past the right or bottom edge
  * repeat the nearest edge sensel of the same colour) and coded as
  * lj92::encode(tile, tile, tile, 2) does (examples/prr2dng/lj92.rs:14-69),
  * byte for byte. tile: even, 2..256 (DNG files use 256); width and height
@@ -532,10 +548,10 @@ typedef struct prr_dng_colour {
     uint8_t pad[6];
 } prr_dng_colour;
 int prr_dng_colour_of(const prr_header* header, prr_dng_colour* out);
-/* Value::srational / Value::rational (examples/prr2dng/tiff.rs:63-98). */
+/* Value::srational / Value::rational (examples/prr2dng/tiff.rs:62-98). */
 int prr_dng_srational(double v, int32_t* num, int32_t* den);
 int prr_dng_rational(double v, uint32_t* num, uint32_t* den);
-/* quicktime_date_time (examples/prr2dng/dng.rs:226-246): UTC text of seconds
+/* quicktime_date_time (examples/prr2dng/dng.rs:211-232): UTC text of seconds
  * since 1904, 19 characters and a NUL; PRR_ERR_BUFFER past the year 9999,
  * whose text would be longer. */
 int prr_dng_date_time(uint64_t seconds, char out[20]);
@@ -546,13 +562,27 @@ int prr_dng_date_time(uint64_t seconds, char out[20]);
  * q always holds 64 entries per block. Device buffers; asynchronous. */
 int prr_transform_blocks(prr_ctx* ctx, int kind, const int16_t* dev_coefs, const int16_t* dev_q,
                          uint16_t* dev_out, size_t nblocks);
-/* decode_component_reduced (src/coefficients.rs:203-312) on the device for
+/* decode_component_reduced (src/coefficients.rs:37-146) on the device for
  * n streams of one packet: stream i at byte dev offset off[i] (alignment =
  * off[i] & 3) of length len[i], writing (64 or 16 or 4) << log2_blocks
  * coefficients per stream (not dequantized). off/len are device arrays. */
 int prr_decode_components(prr_ctx* ctx, const uint8_t* dev_packet, const uint32_t* dev_off,
                           const uint32_t* dev_len, size_t n, int log2_blocks, int log2_coefs,
                           int16_t* dev_coefs);
+/* The same streams through the frame decode's entropy decoder (the one the
+ * full and reduced frame decodes and the batch decode run; the decoder
+ * above is the one inside the fused transform kernels): each stream's
+ * (position, value) list goes to dev_lists (n << (log2_blocks +
+ * log2_coefs) u32, 16-byte aligned), is replayed in order into dev_coefs
+ * as above, and dev_flags[i] = list entries | 1 << 30 when the symbol
+ * budget ran out | 1 << 31 when a zero run wrapped back over stored
+ * positions (then entries past the list's capacity are dropped and the
+ * frame decode decodes the stream again). `staged` != 0: streams are read
+ * from a shared-memory copy of the CTA's span when it fits 32 KB, as in
+ * the frame decode. Same stream semantics as src/coefficients.rs:37-146. */
+int prr_decode_components_events(prr_ctx* ctx, const uint8_t* dev_packet, const uint32_t* dev_off,
+                                 const uint32_t* dev_len, size_t n, int log2_blocks, int log2_coefs,
+                                 int staged, uint32_t* dev_lists, int16_t* dev_coefs, uint32_t* dev_flags);
 
 #ifdef __cplusplus
 }

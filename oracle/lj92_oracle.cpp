@@ -12,7 +12,7 @@
 
 namespace {
 
-// The magnitude category SSSS of a difference: its bit length (lj92.rs:88-91).
+// The magnitude category SSSS of a difference: its bit length (lj92.rs:90-93).
 int category(int32_t d) {
     const uint32_t a = d < 0 ? uint32_t(-int64_t(d)) : uint32_t(d);
     return a == 0 ? 0 : 32 - __builtin_clz(a);
@@ -127,7 +127,7 @@ Table optimal(const uint64_t* histogram) {
 }
 
 // Entropy-coded bits, most significant first, 0xFF bytes stuffed with 0x00
-// (lj92.rs:205-245).
+// (lj92.rs:209-246).
 struct BitWriter {
     std::vector<uint8_t>& out;
     uint64_t buffer = 0;

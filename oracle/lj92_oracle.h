@@ -1,7 +1,7 @@
 /*
  * lj92_oracle.h -- CPU restatement of the DNG export's lossless JPEG tile
  * encoding (examples/prr2dng/lj92.rs and the tile cut of
- * examples/prr2dng/dng.rs:114-125).
+ * examples/prr2dng/dng.rs:115-127).
  *
  * TEST INFRASTRUCTURE ONLY (built into libprr_oracle.so): the checker of
  * the library's device LJ92 encoder, and the timed CPU baseline of the DNG
@@ -9,7 +9,7 @@
  *
  * Parity: the reference is Rust and cannot be built in this image, so no
  * reference-generated streams exist. The restatement is pinned by the
- * reference's own tests of this encoder (lj92.rs:279-399: round trips of
+ * reference's own tests of this encoder (lj92.rs:249-399: round trips of
  * random and extreme samples through a decoder, a flat tile's size bound,
  * the Huffman table of a skewed histogram) run against it, and by a
  * decoder in the tests that reads its streams back to the samples.
@@ -37,7 +37,7 @@ int orc_lj92_encode(const uint16_t* samples, size_t width, size_t height, size_t
 void orc_lj92_huffman(const uint64_t histogram[17], uint8_t counts[16], uint8_t values[17], int* nvalues,
                       uint16_t codes[17], uint8_t lengths[17]);
 
-/* dng::tile (dng.rs:114-125): the tile x tile square at (left, top) of a
+/* dng::tile (dng.rs:115-127): the tile x tile square at (left, top) of a
  * width x height image whose rows are `stride` samples apart; sensels past
  * the right or bottom edge repeat the nearest edge sensel of the same CFA
  * colour. width and height must be at least 2. */

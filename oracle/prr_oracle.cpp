@@ -104,12 +104,12 @@ const uint8_t SCAN_4X4[16] = {0, 4, 1, 5, 8, 12, 9, 13, 2, 6, 3, 7, 10, 14, 11, 
 const uint8_t SCAN_2X2[4] = {0, 2, 1, 3};
 
 inline uint16_t next_cb(const uint16_t* table, size_t n, uint32_t symbol) {
-    return table[std::min<size_t>(symbol, n - 1)];  // coefficients.rs:182-184
+    return table[std::min<size_t>(symbol, n - 1)];  // coefficients.rs:16-18
 }
 
 // ---------------------------------------------------------------------------
 // bits.rs:17-134 -- 64-bit window reader.
-uint32_t partial_word(const uint8_t* b, size_t n) {  // bits.rs:282-288
+uint32_t partial_word(const uint8_t* b, size_t n) {  // bits.rs:31-37
     uint32_t w = 0;
     for (size_t i = 0; i < n && i < 4; i++) w |= uint32_t(b[i]) << (24 - 8 * i);
     return w;
@@ -123,7 +123,7 @@ struct BitReader {
     uint64_t window;
     int32_t extra;
 
-    BitReader(const uint8_t* d, size_t n, size_t align) : data(d), len(n) {  // bits.rs:295-327
+    BitReader(const uint8_t* d, size_t n, size_t align) : data(d), len(n) {  // bits.rs:44-76
         size_t remaining = n;
         size_t address = align;
         uint32_t first;
@@ -150,7 +150,7 @@ struct BitReader {
         words_end = pos + 4 * (remaining / 4);
         window = (uint64_t(first) << 32) | uint64_t(low);
     }
-    uint32_t next_word() {  // bits.rs:330-340
+    uint32_t next_word() {  // bits.rs:79-89
         if (pos < words_end) {
             uint32_t w = be32(data + pos);
             pos += 4;
@@ -161,7 +161,7 @@ struct BitReader {
         return w;
     }
     uint32_t top() const { return uint32_t(window >> 32); }
-    void consume(uint32_t n) {  // bits.rs:348-356
+    void consume(uint32_t n) {  // bits.rs:97-105
         window = window << (n & 63);
         extra = int32_t(uint32_t(extra) - n);
         if (extra < 0) {
@@ -172,7 +172,7 @@ struct BitReader {
     }
 };
 
-// bits.rs:367-385
+// bits.rs:116-134
 inline void codeword(uint32_t p, uint16_t cb, uint32_t& value, uint32_t& len) {
     uint32_t lz = uint32_t(__builtin_clz(p));
     uint32_t s = cb >> 8;
@@ -193,7 +193,7 @@ inline void codeword(uint32_t p, uint16_t cb, uint32_t& value, uint32_t& len) {
     value = ((s + 1) << r) + (p >> ((32u - len) & 31)) - (1u << e);
 }
 
-// coefficients.rs:203-312
+// coefficients.rs:37-146
 void decode_component_reduced(const uint8_t* data, size_t len, size_t align, uint32_t log2_blocks,
                               uint32_t log2_coefs, int16_t* coefs) {
     const uint8_t* scan = log2_coefs == 6 ? SCAN : log2_coefs == 4 ? SCAN_4X4 : SCAN_2X2;

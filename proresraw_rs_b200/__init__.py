@@ -759,6 +759,19 @@ class BatchDecoder:
         _check(_lib.lib().prr_batch_get_config(self.ctx, bucket, C.byref(c)), ctx=self.ctx)
         return BatchConfig._from_c(c)
 
+    def set_wait_limit(self, microseconds: int) -> None:
+        """prr_batch_set_wait_limit: how long a transform segment waits for
+        the entropy chunks of its tiles before its frame reports
+        PRR_ERR_TIMEOUT (0: the 2 s default)."""
+        _check(_lib.lib().prr_batch_set_wait_limit(self.ctx, int(microseconds)), ctx=self.ctx)
+
+    def drop_chunk_for_test(self, chunk: Optional[int]) -> None:
+        """prr_batch_drop_chunk_for_test: from the next batch on, entropy
+        chunk `chunk` is claimed and abandoned, so that the waits on it run
+        out (None: off)."""
+        v = 0xFFFFFFFF if chunk is None else int(chunk)
+        _check(_lib.lib().prr_batch_drop_chunk_for_test(self.ctx, v), ctx=self.ctx)
+
 
 def decode_batch(jobs: Sequence[BatchJob]) -> List[object]:
     """Decode a batch of frames on the current device (see BatchDecoder)."""

@@ -268,9 +268,12 @@ def lib():
                                         P(CError)]),
         "prr_transform_blocks": (i, [vp, i, vp, vp, vp, sz]),
         "prr_decode_components": (i, [vp, vp, vp, vp, sz, i, i, vp]),
+        "prr_decode_components_events": (i, [vp, vp, vp, vp, sz, i, i, i, vp, vp, vp]),
         "prr_decode_noalloc": (i, [i, vp, P(CFrameInfo), vp, i, vp, vp, vp]),
         "prr_batch_submit": (i, [vp, P(CJob), sz]),
         "prr_batch_wait": (i, [vp, C.c_uint32]),
+        "prr_batch_set_wait_limit": (i, [vp, C.c_uint32]),
+        "prr_batch_drop_chunk_for_test": (i, [vp, C.c_uint32]),
         "prr_batch_last_ms": (i, [vp, P(C.c_float)]),
         "prr_batch_bucket": (i, [vp, P(CJob), sz, P(C.c_uint32)]),
         "prr_batch_tune": (i, [vp, P(CJob), sz, C.c_uint32, P(CBatchConfig), P(C.c_float)]),

@@ -666,6 +666,18 @@ int prr_decode_components(prr_ctx* c, const uint8_t* packet, const uint32_t* off
     return c->cuda(launch_decode_components(packet, off, len, n, log2_blocks, log2_coefs, coefs, c->stream));
 }
 
+int prr_decode_components_events(prr_ctx* c, const uint8_t* packet, const uint32_t* off, const uint32_t* len,
+                                 size_t n, int log2_blocks, int log2_coefs, int staged, uint32_t* lists,
+                                 int16_t* coefs, uint32_t* flags) {
+    if (!c || log2_blocks < 0 || log2_blocks > 4 || (log2_coefs != 6 && log2_coefs != 4 && log2_coefs != 2))
+        return PRR_ERR_INVALID;
+    if ((reinterpret_cast<uintptr_t>(packet) & 3) != 0 || (reinterpret_cast<uintptr_t>(lists) & 15) != 0)
+        return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    return c->cuda(launch_decode_components_events(packet, off, len, n, log2_blocks, log2_coefs, staged, lists,
+                                                   coefs, flags, c->stream));
+}
+
 }  // extern "C"
 
 extern "C" int prr_develop_set_occupancy(prr_ctx* c, uint32_t ctas_per_sm) {

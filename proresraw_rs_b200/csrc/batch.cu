@@ -86,6 +86,8 @@ struct BatchState {
     bool pending = false;
     std::vector<FramePlan> plan;
     float last_ms = 0.f;
+    uint32_t wait_limit_us = 0;    // prr_batch_set_wait_limit (0: the 2 s default)
+    uint32_t drop_item = NO_TILE;  // prr_batch_drop_chunk_for_test
 
     // Grow a buffer (by half again at least); a buffer that moves makes the
     // captured graphs stale.
@@ -365,7 +367,9 @@ int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force, c
     hh->nframes = uint32_t(nf);
     hh->ent_items = t.ent_items;
     hh->seg_items = t.seg_items;
-    hh->pad = 0;
+    hh->wait_limit_us = B->wait_limit_us;
+    hh->drop_item = B->drop_item;
+    hh->pad[0] = hh->pad[1] = hh->pad[2] = 0;
     uint32_t ent = 0, seg = 0;
     for (size_t i = 0; i < nf; i++) {
         const FramePlan& f = B->plan[i];
@@ -499,6 +503,24 @@ int prr_batch_bucket(prr_ctx* c, const prr_job* jobs, size_t n, uint32_t* bucket
         tiles += f.ntiles;
     }
     *bucket = bucket_key(nf, tiles);
+    return PRR_OK;
+}
+
+int prr_batch_set_wait_limit(prr_ctx* c, uint32_t microseconds) {
+    if (!c) return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    BatchState* B = nullptr;
+    PRR_TRY(batch_state(c, &B));
+    B->wait_limit_us = microseconds;
+    return PRR_OK;
+}
+
+int prr_batch_drop_chunk_for_test(prr_ctx* c, uint32_t chunk) {
+    if (!c) return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    BatchState* B = nullptr;
+    PRR_TRY(batch_state(c, &B));
+    B->drop_item = chunk;
     return PRR_OK;
 }
 

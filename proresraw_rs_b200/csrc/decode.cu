@@ -290,7 +290,7 @@ __device__ __forceinline__ void seg_scatter(SegShared& S, const FrameDesc& d, ui
         const uint32_t* list = d.pairs + stream_list_base(d, trow, tl.x_rel + S.sq0, tl.log2, s, lc);
         int16_t* base = S.coef + (tl.x_rel * 4 + s) * kCoefStride;
         // Entry: interleaved position n << 16 | raw 16-bit value. Placement
-        // (src/coefficients.rs:252-254) and dequantization (src/idct.rs:41-43)
+        // (src/coefficients.rs:86-88) and dequantization (src/idct.rs:41-43)
         // happen here, off the entropy decoder's serial chain.
         const uint8_t* scan = lc == 6 ? S.T.scan : (lc == 4 ? S.T.scan4 : S.T.scan2);
         const uint32_t hl = lc >> 1, mask = (1u << tl.log2) - 1;
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(kThreads) k_decode_reduced(FrameDesc d, int gr
 // kernel; its list is never written past its capacity. Invalid tiles are
 // left to the transform kernel, which records them.
 //
-// The symbol loop is decode_component_reduced (src/coefficients.rs:203-312)
+// The symbol loop is decode_component_reduced (src/coefficients.rs:37-146)
 // as a state machine, one symbol per iteration; the codebook lookups of all
 // states are issued together and the state's own update picks its result.
 // The 25 distinct codebook parameter sets of the format (src/codebook.rs:25-55).
@@ -572,7 +572,7 @@ __constant__ uint16_t c_cb_params[kCodebooks] = {0x2BC, 0x064, 0x010, 0x021, 0x0
 constexpr uint32_t kIdFirstDc = 0, kIdDcReset = 1, kIdAcInitial = 8, kIdRnInitial = 9, kIdLnInitial = 23;
 
 // Codeword decoding by table. For a view p with lz leading zeros, codeword()
-// (src/bits.rs:367-385) is value = base + ((p << sh1) >> sh2) with a shift of
+// (src/bits.rs:116-134) is value = base + ((p << sh1) >> sh2) with a shift of
 // 32 giving 0, and a length, all fixed by (codebook, lz):
 //   Rice (lz <= s):  base = lz << r, sh1 = (lz + 1) & 31, sh2 = 32 - r,
 //                    length r + 1 + lz;
@@ -657,7 +657,7 @@ struct LeanReader {
     }
 
     __device__ __forceinline__ void init(const Src& s, uint32_t off, uint32_t len) {
-        // BitReader::new (src/bits.rs:295-327).
+        // BitReader::new (src/bits.rs:44-76).
         src = s;
         end = off + len;
         uint32_t remaining = len;
@@ -683,7 +683,7 @@ struct LeanReader {
 
     __device__ __forceinline__ uint32_t top() const { return uint32_t(window >> 32); }
 
-    // BitReader::consume (src/bits.rs:348-356).
+    // BitReader::consume (src/bits.rs:97-105).
     __device__ __forceinline__ void consume(uint32_t n) {
         const bool whole = pos < words_end;
         const uint32_t ww = src.be(pos >> 2);  // independent of n: issued early
@@ -727,7 +727,7 @@ __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off,
     };
     bool live = r.top() != 0;
     // DC: the sign-folded first value, then deltas with a running sign
-    // (src/coefficients.rs:225-248).
+    // (src/coefficients.rs:59-82).
     if (live) {
         uint32_t l;
         const uint32_t v = table_codeword(T, r.top(), kIdFirstDc, l);
@@ -752,7 +752,7 @@ __device__ __forceinline__ uint32_t entropy_events(const Src& src, uint32_t off,
             append(block, uint32_t(dc));
         }
     }
-    // AC (src/coefficients.rs:271-311) as four states, updated with selects
+    // AC (src/coefficients.rs:105-145) as four states, updated with selects
     // so that lanes in different states run the same instructions: the
     // length of a non-zero run, a level inside the run, a zero run, the level
     // after a zero run.
@@ -984,6 +984,72 @@ __global__ void k_decode_components(const uint32_t* __restrict__ words, const ui
                      [&](uint32_t idx, int16_t v) { dst[idx] = v; }, revisited);
 }
 
+// The frame decode's entropy decoder (entropy_events, the one k_entropy and
+// the batch kernel run) on raw streams, so that the crate's component
+// known-answer tests reach it directly. Thread i decodes stream i into its
+// (position, value) list at lists + i * codes, from the packet in global
+// memory or, with `staged` and when the CTA's streams span at most
+// kStageBytes, from a shared-memory stage as k_entropy does; then it replays
+// the list in order into dense coefficients (placement of
+// src/coefficients.rs:86-88), later entries overwriting earlier ones, and
+// writes flags[i] = entry count | bit 30 when the symbol budget ran out |
+// bit 31 when a zero run wrapped back over stored positions.
+template <uint32_t LC>
+__global__ void __launch_bounds__(128) k_decode_components_events(const uint32_t* __restrict__ words,
+                                                                  const uint32_t* __restrict__ off,
+                                                                  const uint32_t* __restrict__ len, size_t n,
+                                                                  uint32_t log2_blocks, int staged,
+                                                                  uint32_t* __restrict__ lists,
+                                                                  int16_t* __restrict__ coefs,
+                                                                  uint32_t* __restrict__ flags) {
+    __shared__ CodeTables CT;
+    __shared__ EntropyTables T;
+    __shared__ __align__(16) uint32_t stage[kStageBytes / 4 + 4];  // + the word after the last byte
+    __shared__ uint32_t s_lo, s_hi;
+    load_tables(&CT);
+    if (threadIdx.x == 0) {
+        s_lo = 0xFFFFFFFFu;
+        s_hi = 0;
+    }
+    __syncthreads();
+    build_entropy_tables(T, CT);
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool mine = i < n;
+    const uint32_t o = mine ? off[i] : 0, l = mine ? len[i] : 0;
+    if (mine) {
+        atomicMin(&s_lo, o);
+        atomicMax(&s_hi, o + l);
+    }
+    __syncthreads();
+    const uint32_t base = s_lo & ~15u, top = (s_hi + 15) & ~15u;
+    const bool use_stage = staged && s_lo <= s_hi && top - base <= kStageBytes;
+    if (use_stage) {
+        const uint4* src = reinterpret_cast<const uint4*>(words) + base / 16;
+        uint4* dst = reinterpret_cast<uint4*>(stage);
+        for (uint32_t k = threadIdx.x; k < (top - base) / 16; k += blockDim.x) {
+            const uint4 v = __ldg(src + k);
+            dst[k] = make_uint4(bswap32(v.x), bswap32(v.y), bswap32(v.z), bswap32(v.w));
+        }
+    }
+    __syncthreads();
+    if (!mine) return;
+    const uint32_t codes = 1u << (log2_blocks + LC);
+    uint32_t* list = lists + i * codes;
+    bool revisited = false, ok = true;
+    const uint32_t cnt =
+        use_stage ? entropy_events<LC>(StagedWords{stage, base >> 2}, o, l, log2_blocks, T, list, revisited, ok)
+                  : entropy_events<LC>(PacketWords{words}, o, l, log2_blocks, T, list, revisited, ok);
+    int16_t* dst = coefs + i * codes;
+    for (uint32_t k = 0; k < codes; k++) dst[k] = 0;
+    const uint8_t* scan = LC == 6 ? CT.scan : (LC == 4 ? CT.scan4 : CT.scan2);
+    const uint32_t mask = (1u << log2_blocks) - 1;
+    for (uint32_t k = 0; k < cnt; k++) {
+        const uint32_t e = list[k], nn = e >> 16;
+        dst[((nn & mask) << LC) + scan[nn >> log2_blocks]] = int16_t(e & 0xFFFF);
+    }
+    flags[i] = cnt | (ok ? 0u : 0x40000000u) | (revisited ? 0x80000000u : 0u);
+}
+
 // ---------------------------------------------------------------------------
 // Batch decode: one CTA per frame for the tile offsets, then one persistent
 // launch for the entropy chunks and transform segments of all frames.
@@ -1140,6 +1206,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
     build_entropy_tables(T, S.T);
     const uint32_t nframes = b.hdr->nframes, ent_items = b.hdr->ent_items;
     const uint32_t total = ent_items + b.hdr->seg_items;
+    const uint32_t drop_item = b.hdr->drop_item;
+    const uint64_t wait_ns = b.hdr->wait_limit_us ? uint64_t(b.hdr->wait_limit_us) * 1000u : kChunkWaitNs;
     for (;;) {
         __syncthreads();  // the previous item's shared memory is no longer read
         if (tid == 0) {
@@ -1157,6 +1225,10 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
         for (uint32_t i = tid; i < sizeof(FrameDesc) / 4; i += kBatchThreads)
             reinterpret_cast<uint32_t*>(&fd)[i] = reinterpret_cast<const uint32_t*>(&F.d)[i];
         const uint32_t shift = F.shift, lc = F.lc, greens = F.greens;
+        // A test can name one chunk that is claimed and then abandoned, as a
+        // CTA that died would leave it: its flag is never set, and the
+        // segments that wait for it give up after wait_ns.
+        if (item == drop_item && item < ent_items) continue;
         if (item < ent_items) {
             __syncthreads();
             const uint32_t chunk = item - F.ent_begin;
@@ -1185,7 +1257,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
             const uint32_t last = trow * F.d.tiles_per_row + min(j0 + 15, F.d.tiles_per_row - 1);
             bool ok = true;
             for (uint32_t c = first / kBatchTilesPerChunk; ok && c <= last / kBatchTilesPerChunk; c++)
-                ok = wait_flag(b.flags + F.ent_begin + c, s_epoch, kChunkWaitNs);
+                ok = wait_flag(b.flags + F.ent_begin + c, s_epoch, wait_ns);
             if (!ok) {
                 atomicOr(&b.q->error, 1u);
                 atomicOr(&F.st->error, 2u);
@@ -1369,6 +1441,23 @@ cudaError_t launch_decode_components(const uint8_t* packet, const uint32_t* off,
     const unsigned blocks = unsigned((n + 63) / 64);
     k_decode_components<<<blocks, 64, 0, s>>>(reinterpret_cast<const uint32_t*>(packet), off, len, n,
                                               log2_blocks, log2_coefs, coefs);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_decode_components_events(const uint8_t* packet, const uint32_t* off, const uint32_t* len,
+                                            size_t n, int log2_blocks, int log2_coefs, int staged,
+                                            uint32_t* lists, int16_t* coefs, uint32_t* flags, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const unsigned blocks = unsigned((n + 127) / 128);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(packet);
+    const uint32_t lb = uint32_t(log2_blocks);
+    if (log2_coefs == 6)
+        k_decode_components_events<6><<<blocks, 128, 0, s>>>(w, off, len, n, lb, staged, lists, coefs, flags);
+    else if (log2_coefs == 4)
+        k_decode_components_events<4><<<blocks, 128, 0, s>>>(w, off, len, n, lb, staged, lists, coefs, flags);
+    else
+        k_decode_components_events<2><<<blocks, 128, 0, s>>>(w, off, len, n, lb, staged, lists, coefs, flags);
     count_launch();
     return cudaGetLastError();
 }

@@ -315,7 +315,7 @@ struct DevShared {
 };
 
 // White balance, clip and output matrix of a row's two sites as the lanes
-// of pairs (src/demosaic.rs:682-720).
+// of pairs (src/demosaic.rs:683-720).
 __device__ __forceinline__ void finish_x2(float2 r, float2 g, float2 b, const DevelopDesc& d, float2* out) {
     float2 rr = mul2(r, bc(d.wb[0]));
     float2 bb = mul2(b, bc(d.wb[1]));

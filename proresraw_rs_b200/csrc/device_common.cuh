@@ -132,7 +132,7 @@ struct Reader {
         }
     }
 
-    // BitReader::new (src/bits.rs:295-327) for `len` bytes at packet offset
+    // BitReader::new (src/bits.rs:44-76) for `len` bytes at packet offset
     // `off`; the stream's alignment is off & 3 (the packet counts as aligned,
     // src/decoder.rs:288-291).
     __device__ __forceinline__ void init(const Src& s, uint32_t off, uint32_t len) {
@@ -166,7 +166,7 @@ struct Reader {
 
     __device__ __forceinline__ uint32_t top() const { return uint32_t(window >> 32); }
 
-    // BitReader::consume (src/bits.rs:348-356): drop n bits, refilling at
+    // BitReader::consume (src/bits.rs:97-105): drop n bits, refilling at
     // most once.
     __device__ __forceinline__ void consume(uint32_t n) {
         window <<= (n & 63);
@@ -180,7 +180,7 @@ struct Reader {
     }
 };
 
-// codeword, src/bits.rs:367-385, for a view p != 0: value and length. The
+// codeword, src/bits.rs:116-134, for a view p != 0: value and length. The
 // Rice and exp-Golomb results are both computed and one is selected, so
 // lanes decoding different kinds of codeword do not diverge. (The crate's
 // separate branch for a set top bit is the Rice case with no leading zero.)
@@ -198,7 +198,7 @@ __device__ __forceinline__ uint32_t codeword(uint32_t p, uint32_t cb, uint32_t& 
     return rice ? rice_val : eg_val;
 }
 
-// decode_component_reduced, src/coefficients.rs:203-312, as a state machine
+// decode_component_reduced, src/coefficients.rs:37-146, as a state machine
 // that decodes one symbol per iteration: the DC fold, the DC deltas, the
 // non-zero run length, the levels of a run, the zero run and the level after
 // it. Every lane of a warp runs the same codeword and consume for its own
@@ -233,7 +233,7 @@ __device__ __forceinline__ bool decode_component(const Src& src, uint32_t off, u
         uint32_t l;
         const uint32_t v = codeword(top, cb, l);
         const bool is_level = state == LEVELS || state == LEVEL;
-        // A level's sign is the bit after its codeword (src/coefficients.rs:256-270).
+        // A level's sign is the bit after its codeword (src/coefficients.rs:90-104).
         const bool negative = int32_t(top << (l & 31)) < 0;
         r.consume(l + (is_level ? 1u : 0u));
         if (is_level) {

@@ -68,7 +68,7 @@ Value srationals(const std::vector<std::pair<int32_t, int32_t>>& xs) {
     return v;
 }
 
-// Value::srational (tiff.rs:63-80): the closest signed rational with a
+// Value::srational (tiff.rs:62-79): the closest signed rational with a
 // power-of-ten denominator of at most 10^6.
 std::pair<int32_t, int32_t> srational(double v) {
     int64_t d = 1000000;
@@ -79,7 +79,7 @@ std::pair<int32_t, int32_t> srational(double v) {
     return {int32_t(c), int32_t(d)};
 }
 
-// Value::rational (tiff.rs:82-98), for non-negative values.
+// Value::rational (tiff.rs:81-98), for non-negative values.
 std::pair<uint32_t, uint32_t> rational(double v) {
     uint64_t d = 1000000;
     while (d > 1 && v * double(d) >= double(UINT32_MAX)) d /= 10;
@@ -184,7 +184,7 @@ V3 apply(const M3& m, const V3& v) {
     return r;
 }
 M3 diag(const V3& v) { return M3{{{v.v[0], 0.0, 0.0}, {0.0, v.v[1], 0.0}, {0.0, 0.0, v.v[2]}}}; }
-// The inverse by cofactors (colour.rs:196-205).
+// The inverse by cofactors (colour.rs:171-179).
 M3 inverse(const M3& a) {
     auto cof = [&](int r, int c) {
         const int r0 = (r + 1) % 3, r1 = (r + 2) % 3, c0 = (c + 1) % 3, c1 = (c + 2) % 3;
@@ -216,7 +216,7 @@ XY daylight_xy(double t) {
     return XY{x, -3.0 * x * x + 2.870 * x - 0.275};
 }
 XY white_xy(double t) { return t < 4000.0 ? planck_xy(t) : daylight_xy(t); }
-// Bradford adaptation from white `from` to white `to` (colour.rs:176-182).
+// Bradford adaptation from white `from` to white `to` (colour.rs:151-156).
 M3 bradford(XY from, XY to) {
     const V3 s = apply(kBradford, xyz(from)), d = apply(kBradford, xyz(to));
     const V3 gains{{d.v[0] / s.v[0], d.v[1] / s.v[1], d.v[2] / s.v[2]}};
@@ -225,7 +225,7 @@ M3 bradford(XY from, XY to) {
 
 double gain(float g) { return g > 0.0f && std::isfinite(g) ? double(g) : 1.0; }
 
-// DngColour::new (colour.rs:78-119).
+// DngColour::new (colour.rs:74-111).
 prr_dng_colour colour_of(const prr_header& h) {
     prr_dng_colour c{};
     const double temperature = h.wb_cct == 0 ? 6504.0 : std::fmin(std::fmax(double(h.wb_cct), 1000.0), 25000.0);
@@ -256,7 +256,7 @@ prr_dng_colour colour_of(const prr_header& h) {
     return c;
 }
 
-// --- the DNG tags (dng.rs:128-223) ------------------------------------------
+// --- the DNG tags (dng.rs:138-209) ------------------------------------------
 
 // Curve::linearize (src/curve.rs:14-24).
 uint16_t linearize(const uint16_t* curve, uint32_t code) {
@@ -463,7 +463,7 @@ int prr_dng_rational(double v, uint32_t* num, uint32_t* den) {
     return PRR_OK;
 }
 
-// quicktime_date_time (dng.rs:226-246): days from 1904-01-01 to the Unix
+// quicktime_date_time (dng.rs:211-232): days from 1904-01-01 to the Unix
 // epoch, then the civil date of a Unix day (Howard Hinnant's algorithm).
 int prr_dng_date_time(uint64_t seconds, char out[20]) {
     if (!out) return PRR_ERR_INVALID;

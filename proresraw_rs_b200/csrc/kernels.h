@@ -83,9 +83,11 @@ struct BatchQueue {
 // (or one captured graph) serves every batch that fits the buffers.
 struct BatchHeader {
     uint32_t nframes;
-    uint32_t ent_items;  // chunks of all frames
-    uint32_t seg_items;  // segments of all frames
-    uint32_t pad;
+    uint32_t ent_items;      // chunks of all frames
+    uint32_t seg_items;      // segments of all frames
+    uint32_t wait_limit_us;  // a segment's wait for a chunk flag (0: kChunkWaitNs)
+    uint32_t drop_item;      // a chunk claimed but never decoded nor flagged (tests), or NO_TILE
+    uint32_t pad[3];
 };
 
 struct BatchDesc {
@@ -113,6 +115,10 @@ cudaError_t launch_transform_blocks(int kind, const int16_t* coefs, const int16_
 cudaError_t launch_decode_components(const uint8_t* packet, const uint32_t* off,
                                      const uint32_t* len, size_t n, int log2_blocks,
                                      int log2_coefs, int16_t* coefs, cudaStream_t s);
+cudaError_t launch_decode_components_events(const uint8_t* packet, const uint32_t* off,
+                                            const uint32_t* len, size_t n, int log2_blocks, int log2_coefs,
+                                            int staged, uint32_t* lists, int16_t* coefs, uint32_t* flags,
+                                            cudaStream_t s);
 
 // Develop / linearize.
 struct DevelopDesc {

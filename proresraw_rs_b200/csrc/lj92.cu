@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(kLjThreads, 1) k_lj92_encode(Lj92Desc d) {
     }
     __syncthreads();
     if (threadIdx.x == 0 && (total_bits & 7)) {
-        // Pad the last byte with one bits (lj92.rs:238-244).
+        // Pad the last byte with one bits (lj92.rs:239-245).
         const uint32_t used = uint32_t(total_bits % 32), pad = 8 - uint32_t(total_bits & 7);
         words[total_bits / 32] |= ((1u << pad) - 1) << (32 - used - pad);
     }

@@ -240,7 +240,7 @@ std::string lossy_utf8(const uint8_t* p, size_t n) {
 }
 
 // The UTF-8 items of a `meta` atom whose keys use the `mdta` namespace
-// (src/mov.rs:597-640).
+// (src/mov.rs:598-640).
 std::vector<std::pair<std::string, std::string>> text_metadata(Span meta) {
     Span body;
     if (meta.n >= 8 && std::memcmp(meta.p + 4, "hdlr", 4) == 0) {

@@ -31,8 +31,9 @@ void* g_scratch[kMaxDevices] = {};
 // The device address of g_tile_off on `device`, looked up once per device
 // with that device current. Host code cannot pass &g_tile_off to a kernel:
 // on the host the name stands for a host-side shadow, not device memory.
+// The cached address belongs to the device's primary context; it is not
+// valid after cudaDeviceReset (the library does not support that).
 int scratch_for(int device, uint32_t** out) {
-    if (device < 0 || device >= kMaxDevices) return PRR_ERR_INVALID;
     std::lock_guard<std::mutex> lock(g_mutex);
     if (!g_scratch[device]) {
         void* p = nullptr;
@@ -46,26 +47,46 @@ int scratch_for(int device, uint32_t** out) {
     return PRR_OK;
 }
 
-}  // namespace
-
-extern "C" int prr_decode_noalloc(int device, void* cuda_stream, const prr_frame_info* info,
-                                  const uint8_t* dev_packet, int idct, uint16_t* dev_samples,
-                                  prr_dev_status* dev_status, uint32_t* dev_skipped) {
-    if (!info || !dev_packet || !dev_samples || !dev_status || !dev_skipped) return PRR_ERR_INVALID;
-    if ((reinterpret_cast<uintptr_t>(dev_packet) & 3) != 0) return PRR_ERR_INVALID;
-    if (idct != PRR_IDCT_APPLE && idct != PRR_IDCT_FFMPEG) return PRR_ERR_INVALID;
-    if (info->ntiles > kMaxTiles) return PRR_ERR_SCRATCH_LIMIT;
-    if (cudaSetDevice(device) != cudaSuccess) {
-        cudaGetLastError();
-        return PRR_ERR_CUDA;
-    }
+// The decode proper, with `device` current.
+int decode_on_device(int device, cudaStream_t s, const prr_frame_info* info, const uint8_t* dev_packet,
+                     int idct, uint16_t* dev_samples, prr_dev_status* dev_status, uint32_t* dev_skipped) {
     uint32_t* tile_off = nullptr;
     const int rc = scratch_for(device, &tile_off);
     if (rc != PRR_OK) return rc;
-    cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
     const prr::FrameDesc d = prr::make_frame_desc(*info, dev_packet);
     if (prr::launch_tile_index(d, tile_off, dev_status, s) != cudaSuccess) return PRR_ERR_CUDA;
     if (prr::launch_decode_full(d, idct, tile_off, dev_status, dev_skipped, dev_samples, s) != cudaSuccess)
         return PRR_ERR_CUDA;
     return PRR_OK;
+}
+
+}  // namespace
+
+extern "C" int prr_decode_noalloc(int device, void* cuda_stream, const prr_frame_info* info,
+                                  const uint8_t* dev_packet, int idct, uint16_t* dev_samples,
+                                  prr_dev_status* dev_status, uint32_t* dev_skipped) {
+    // Argument checks come before any CUDA call.
+    if (device < 0 || device >= kMaxDevices) return PRR_ERR_INVALID;
+    if (!info || !dev_packet || !dev_samples || !dev_status || !dev_skipped) return PRR_ERR_INVALID;
+    if ((reinterpret_cast<uintptr_t>(dev_packet) & 3) != 0) return PRR_ERR_INVALID;
+    if (idct != PRR_IDCT_APPLE && idct != PRR_IDCT_FFMPEG) return PRR_ERR_INVALID;
+    if (info->ntiles > kMaxTiles) return PRR_ERR_SCRATCH_LIMIT;
+    // The caller's current device is put back before returning: a plug-in
+    // host that owns the device context keeps its own current device.
+    int caller = -1;
+    if (cudaGetDevice(&caller) != cudaSuccess) {
+        cudaGetLastError();
+        return PRR_ERR_CUDA;
+    }
+    if (caller != device && cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return PRR_ERR_CUDA;
+    }
+    const int rc = decode_on_device(device, static_cast<cudaStream_t>(cuda_stream), info, dev_packet, idct,
+                                    dev_samples, dev_status, dev_skipped);
+    if (caller != device && cudaSetDevice(caller) != cudaSuccess) {
+        cudaGetLastError();
+        return rc != PRR_OK ? rc : PRR_ERR_CUDA;
+    }
+    return rc;
 }

@@ -110,21 +110,21 @@ def _header_c(header) -> _lib.CHeader:
 
 
 def srational(v: float) -> Tuple[int, int]:
-    """Value::srational (tiff.rs:63-80) of one value."""
+    """Value::srational (tiff.rs:62-79) of one value."""
     n, d = C.c_int32(), C.c_int32()
     _lib.lib().prr_dng_srational(float(v), C.byref(n), C.byref(d))
     return n.value, d.value
 
 
 def rational(v: float) -> Tuple[int, int]:
-    """Value::rational (tiff.rs:82-98) of one value."""
+    """Value::rational (tiff.rs:81-98) of one value."""
     n, d = C.c_uint32(), C.c_uint32()
     _lib.lib().prr_dng_rational(float(v), C.byref(n), C.byref(d))
     return n.value, d.value
 
 
 def quicktime_date_time(seconds: int) -> str:
-    """dng.rs:226-246: UTC `YYYY:MM:DD HH:MM:SS` of a QuickTime time."""
+    """dng.rs:211-232: UTC `YYYY:MM:DD HH:MM:SS` of a QuickTime time."""
     buf = C.create_string_buffer(20)
     rc = _lib.lib().prr_dng_date_time(int(seconds), buf)
     if rc:

@@ -1,6 +1,6 @@
 """Hand-built QuickTime movies: the atoms a video track's sample table is
 read from, written the way the crate's own tests build theirs
-(src/mov.rs:808-995), plus clips whose samples are real frame packets.
+(src/mov.rs:810-995), plus clips whose samples are real frame packets.
 
 Used by the tests of the movie reader and by the clip benchmark (a movie of
 synthetic frames on local disk, since no camera clip is available).

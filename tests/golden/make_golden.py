@@ -7,14 +7,17 @@ little-endian, and tests/data/idct_hash.txt, the FNV-1a hash of the outputs
 of 2^20 blocks from testgen::Gen(0x4a54). They are data, copied verbatim so
 the tests can run where the reference tree is absent.
 
-Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT
+(REFERENCE_ROOT: the proresraw_rs checkout, the directory holding tests/data/)
 """
 import hashlib
 import pathlib
 import shutil
 import sys
 
-root = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    sys.exit("usage: make_golden.py REFERENCE_ROOT")
+root = pathlib.Path(sys.argv[1])
 here = pathlib.Path(__file__).resolve().parent
 for name in ["idct_vectors.bin", "idct_hash.txt"]:
     src = root / "tests" / "data" / name

@@ -180,3 +180,31 @@ def test_submit_twice_or_wait_without_submit_is_invalid(corpus):
     assert e.value.code == P._lib.ERR_INVALID
     for job, g in zip(jobs, dec.wait()):
         assert_job(job, g, oracle_of(job))
+
+
+def test_a_chunk_that_never_finishes_times_out_and_the_context_stays_usable():
+    """A bounded device wait that runs out. The test hook abandons the first
+    entropy chunk of the batch, so its flag is never set: the segments of
+    the first frame that wait for it give up after the (shortened) limit,
+    that frame reports PRR_ERR_TIMEOUT, the other frames are still exact,
+    and the next batch on the same context is exact too."""
+    import time
+
+    items = S.mixed_batch(6, seed=7, sizes=SMALL_SIZES, corrupt=0.0)
+    jobs = jobs_of(items)
+    wants = [oracle_of(j) for j in jobs]
+    assert not isinstance(wants[0], O.OracleError)
+    dec = P.BatchDecoder()
+    dec.set_wait_limit(20_000)  # 20 ms
+    dec.drop_chunk_for_test(0)
+    t0 = time.perf_counter()
+    got = dec.decode(jobs)
+    elapsed = time.perf_counter() - t0
+    assert isinstance(got[0], P.Error) and got[0].code == P._lib.ERR_TIMEOUT, got[0]
+    for job, g, w in zip(jobs[1:], got[1:], wants[1:]):
+        assert_job(job, g, w)
+    assert elapsed < 10.0  # the waits ended after their limit, not after the 2 s default
+    dec.drop_chunk_for_test(None)
+    dec.set_wait_limit(0)
+    for job, g, w in zip(jobs, dec.decode(jobs), wants):
+        assert_job(job, g, w)

@@ -119,6 +119,74 @@ def test_entropy_decode_matches_the_oracle_on_random_streams(log2_coefs):
             assert np.array_equal(got[i], want), (log2_blocks, i)
 
 
+def decode_components_events_dev(data: bytes, offs, lens, log2_blocks, log2_coefs, staged):
+    """prr_decode_components_events: the frame decode's entropy decoder
+    (entropy_events) on raw streams. Returns the dense coefficients and the
+    per-stream flags (entry count | bit 30 budget ran out | bit 31 wrapped)."""
+    t = torch()
+    buf = np.zeros(P._lib.lib().prr_padded_packet_bytes(len(data)), dtype=np.uint8)
+    buf[: len(data)] = np.frombuffer(data, dtype=np.uint8)
+    d = dev(buf)
+    o, ln = dev(np.array(offs, dtype=np.uint32)), dev(np.array(lens, dtype=np.uint32))
+    codes = 1 << (log2_blocks + log2_coefs)
+    lists = t.full((len(offs) * codes,), -1, dtype=t.int32, device="cuda")
+    out = t.full((len(offs) * codes,), 0x5A5A, dtype=t.int16, device="cuda")
+    flags = t.zeros(len(offs), dtype=t.int32, device="cuda")
+    rc = _lib.lib().prr_decode_components_events(P.context(), d.data_ptr(), o.data_ptr(), ln.data_ptr(), len(offs),
+                                                 log2_blocks, log2_coefs, int(staged), lists.data_ptr(),
+                                                 out.data_ptr(), flags.data_ptr())
+    assert rc == 0
+    t.cuda.synchronize()
+    return out.cpu().numpy().reshape(len(offs), codes), flags.cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize("staged", [False, True], ids=["global", "staged"])
+@pytest.mark.parametrize("case", _coef_cases(), ids=lambda c: c[0])
+def test_coefficient_kats_through_the_frame_entropy_decoder(case, staged):
+    # The crate's component KATs (src/coefficients.rs:150-229) on the
+    # decoder the frame, reduced and batch decodes run.
+    _, data, log2, check = case
+    got, flags = decode_components_events_dev(data, [0], [len(data)], log2, 6, staged)
+    assert flags[0] >> 30 == 0
+    assert check(got[0])
+    assert np.array_equal(got[0], O.decode_component(data, 0, log2))
+
+
+@pytest.mark.parametrize("staged", [False, True], ids=["global", "staged"])
+def test_the_frame_entropy_decoder_flags_a_wrapped_zero_run(staged):
+    stream = wrapped_zero_run_stream()
+    got, flags = decode_components_events_dev(stream, [0], [len(stream)], 0, 6, staged)
+    assert flags[0] >> 31 == 1  # the frame decode replays this stream in order
+    # Few enough entries that none was dropped: the in-order replay is exact.
+    assert flags[0] & 0x3FFFFFFF < 64
+    assert np.array_equal(got[0], O.decode_component(stream, 0, 0))
+
+
+@pytest.mark.parametrize("staged", [False, True], ids=["global", "staged"])
+@pytest.mark.parametrize("log2_coefs", [6, 4, 2])
+def test_the_frame_entropy_decoder_matches_the_oracle_on_random_streams(log2_coefs, staged):
+    rng = np.random.default_rng(170 + log2_coefs)
+    for log2_blocks in range(5):
+        n = 384
+        lens = rng.integers(0, 48 * (1 << log2_blocks) + 1, n)
+        data = bytearray()
+        offs = []
+        for i in range(n):
+            offs.append(len(data))
+            raw = rng.integers(0, 256, (2, int(lens[i])), dtype=np.uint8)
+            data += (raw[0] & raw[1]).tobytes()
+            data += bytes(int(rng.integers(0, 4)))  # vary the 4-byte alignment
+        data = bytes(data)
+        got, flags = decode_components_events_dev(data, offs, lens.tolist(), log2_blocks, log2_coefs, staged)
+        codes = 1 << (log2_blocks + log2_coefs)
+        for i in range(n):
+            assert flags[i] >> 30 & 1 == 0
+            if flags[i] >> 31 and flags[i] & 0x3FFFFFFF == codes:
+                continue  # entries may have been dropped; the frame decode decodes it again
+            want = O.decode_component(data[offs[i]: offs[i] + int(lens[i])], offs[i] & 3, log2_blocks, log2_coefs)
+            assert np.array_equal(got[i], want), (log2_blocks, i)
+
+
 def assert_frames_equal(pkt, idct=0):
     o = O.decode_frame(pkt, idct)
     g = P.decode_frame_with(pkt, P.Idct(idct))

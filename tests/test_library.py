@@ -64,3 +64,15 @@ def test_clip_calls_refuse_a_null_pipeline():
     assert L.prr_clip_start(None, 0, 1, _lib.SCALE_FULL, 0, 0) == _lib.ERR_INVALID
     assert L.prr_clip_queue(None, 0, 1, _lib.SCALE_FULL, 0, 0) == _lib.ERR_INVALID
     assert L.prr_clip_next(None, None) == _lib.ERR_INVALID
+
+
+def test_noalloc_refuses_device_ordinals_out_of_range_before_any_cuda_call():
+    # prr_decode_noalloc checks its arguments before it touches CUDA, so a
+    # device ordinal outside [0, 64) is refused even without a device.
+    L = _lib.lib()
+    info = _lib.CFrameInfo()
+    p = C.c_void_p(16)  # never dereferenced: the call returns first
+    for device in (-1, 64, 1 << 20):
+        assert L.prr_decode_noalloc(device, None, C.byref(info), p, 0, p, p, p) == _lib.ERR_INVALID
+    info.ntiles = _lib.NOALLOC_MAX_TILES + 1
+    assert L.prr_decode_noalloc(0, None, C.byref(info), p, 0, p, p, p) == _lib.ERR_SCRATCH_LIMIT

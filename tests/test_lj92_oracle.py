@@ -1,6 +1,6 @@
 """The CPU oracle of the DNG export's lossless JPEG encoder, pinned by the
-reference's own tests of it (examples/prr2dng/lj92.rs:372-399,
-examples/prr2dng/dng.rs:243-254): round trips through a decoder, a flat
+reference's own tests of it (examples/prr2dng/lj92.rs:340-399,
+examples/prr2dng/dng.rs:238-248): round trips through a decoder, a flat
 tile's size, the Huffman table of a skewed histogram, the tile cut's edge
 padding. CPU only."""
 
