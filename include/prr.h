@@ -373,6 +373,31 @@ int prr_sg_gradients(prr_ctx* ctx, const float* in16, const float* base3, const 
  * find room on every SM while this context's develop runs. */
 int prr_develop_set_occupancy(prr_ctx* ctx, uint32_t ctas_per_sm);
 
+/* Launch shape of the develop kernel, per bucket of frame sizes: the
+ * output tile (32x32, the default; 32x16; 64x16) and the CTAs per SM (0: as
+ * many as fit). Every shape gives the same output bit for bit. The
+ * crate's analogous knob is GpuDeveloper::set_band_rows
+ * (src/gpu/develop.rs:44,281); a tile shape replaces its band height. */
+typedef struct prr_develop_config {
+    uint32_t tile_w, tile_h;
+    uint32_t ctas_per_sm;
+} prr_develop_config;
+/* The bucket of a frame size: (ceil log2 width) << 8 | ceil log2 height. */
+uint32_t prr_develop_bucket(uint32_t width, uint32_t height);
+/* Use `cfg` for the frames of `bucket` (PRR_ERR_INVALID for a shape not
+ * listed above). prr_develop_set_occupancy, when nonzero, still caps the
+ * CTAs per SM. */
+int prr_develop_set_config(prr_ctx* ctx, uint32_t bucket, const prr_develop_config* cfg);
+/* The config of `bucket` (the default when none was set or tuned). */
+int prr_develop_get_config(prr_ctx* ctx, uint32_t bucket, prr_develop_config* cfg);
+/* Autotuner: develop this frame (arguments as prr_develop; the outputs are
+ * written) with every candidate shape, `reps` timed runs each after an
+ * untimed one, and keep the fastest (median device time) as the config of
+ * the frame's bucket. Synchronous. */
+int prr_develop_tune(prr_ctx* ctx, const prr_header* header, const prr_params* params, int stage,
+                     const uint16_t* dev_samples, int layout, float* r, float* g, float* b,
+                     size_t out_len, uint32_t reps, prr_develop_config* best, float* best_ms);
+
 /* --- host-buffer conveniences (synchronous) ----------------------------------- */
 /* decode_frame_with + develop_planar_into / develop_into with host input and
  * host outputs: uploads the packet, decodes and develops on the device and

@@ -603,6 +603,59 @@ def develop_planar_into(frame: Frame, params: DemosaicParams, stage: Stage, out:
     _develop(frame, params, stage, 1, list(out))
 
 
+@dataclasses.dataclass
+class DevelopConfig:
+    """Launch shape of the develop kernel (prr_develop_config): output tile
+    32x32 (default), 32x16 or 64x16, and CTAs per SM (0: as many as fit)."""
+    tile_w: int = 32
+    tile_h: int = 32
+    ctas_per_sm: int = 0
+
+    def _c(self) -> _lib.CDevelopConfig:
+        return _lib.CDevelopConfig(self.tile_w, self.tile_h, self.ctas_per_sm)
+
+    @staticmethod
+    def _from_c(c: _lib.CDevelopConfig) -> "DevelopConfig":
+        return DevelopConfig(int(c.tile_w), int(c.tile_h), int(c.ctas_per_sm))
+
+
+def develop_bucket(width: int, height: int) -> int:
+    """The frame-size bucket the develop's launch shape is kept for."""
+    return int(_lib.lib().prr_develop_bucket(width, height))
+
+
+def develop_set_config(bucket: int, cfg: DevelopConfig) -> None:
+    """Use `cfg` for the frames of `bucket` (current device and stream)."""
+    ctx = context()
+    c = cfg._c()
+    _check(_lib.lib().prr_develop_set_config(ctx, bucket, C.byref(c)), ctx=ctx)
+
+
+def develop_get_config(bucket: int) -> DevelopConfig:
+    ctx = context()
+    c = _lib.CDevelopConfig()
+    _check(_lib.lib().prr_develop_get_config(ctx, bucket, C.byref(c)), ctx=ctx)
+    return DevelopConfig._from_c(c)
+
+
+def develop_tune(frame: Frame, params: DemosaicParams, stage: Stage, out: Sequence,
+                 reps: int = 3) -> Tuple[DevelopConfig, float]:
+    """prr_develop_tune: develop `frame` into the device planes `out` (3
+    planes, or one interleaved buffer) with every candidate launch shape;
+    the fastest becomes the config of the frame's size bucket. Returns
+    (config, median ms)."""
+    w, h = frame.width(), frame.height()
+    layout = 1 if len(out) == 3 else 0
+    want = w * h if layout == 1 else 3 * w * h
+    ctx = context(frame.samples.device.index)
+    ptrs = [_dptr(o) for o in out] + [None] * (3 - len(out))
+    best, ms = _lib.CDevelopConfig(), C.c_float()
+    _check(_lib.lib().prr_develop_tune(ctx, C.byref(frame.header._c), C.byref(params._c()), int(stage),
+                                       _dptr(frame.samples), layout, ptrs[0], ptrs[1], ptrs[2], want, reps,
+                                       C.byref(best), C.byref(ms)), ctx=ctx)
+    return DevelopConfig._from_c(best), float(ms.value)
+
+
 # ---------------------------------------------------------------------------
 # Batched decode (prr_batch_* in include/prr.h): many frames of any mix of
 # sizes, versions, patterns, qscales and alignments, full or reduced, in one
@@ -784,5 +837,6 @@ __all__ = [
     "parse_frame", "frame_info", "frame_quantizer", "context", "kernel_launches", "Frame", "decode_frame",
     "decode_frame_with", "RgbFrame", "decode_frame_reduced", "decode_frame_reduced_with", "DemosaicParams",
     "output_matrix", "RgbImage", "RgbPlanes", "develop", "develop_with", "develop_into", "develop_planar",
-    "develop_planar_into", "BatchJob", "BatchConfig", "BatchDecoder", "decode_batch",
+    "develop_planar_into", "DevelopConfig", "develop_bucket", "develop_set_config", "develop_get_config",
+    "develop_tune", "BatchJob", "BatchConfig", "BatchDecoder", "decode_batch",
 ]

@@ -133,6 +133,14 @@ class CJob(C.Structure):
     ]
 
 
+class CDevelopConfig(C.Structure):
+    _fields_ = [
+        ("tile_w", C.c_uint32),
+        ("tile_h", C.c_uint32),
+        ("ctas_per_sm", C.c_uint32),
+    ]
+
+
 class CBatchConfig(C.Structure):
     _fields_ = [
         ("ctas_per_sm", C.c_uint32),
@@ -264,6 +272,11 @@ def lib():
         "prr_output_matrix": (i, [P(CHeader), i, vp]),
         "prr_develop": (i, [vp, P(CHeader), P(CParams), i, vp, i, vp, vp, vp, sz]),
         "prr_develop_set_occupancy": (i, [vp, C.c_uint32]),
+        "prr_develop_bucket": (C.c_uint32, [C.c_uint32, C.c_uint32]),
+        "prr_develop_set_config": (i, [vp, C.c_uint32, P(CDevelopConfig)]),
+        "prr_develop_get_config": (i, [vp, C.c_uint32, P(CDevelopConfig)]),
+        "prr_develop_tune": (i, [vp, P(CHeader), P(CParams), i, vp, i, vp, vp, vp, sz, C.c_uint32,
+                                 P(CDevelopConfig), P(C.c_float)]),
         "prr_decode_develop_host": (i, [vp, vp, sz, i, P(CParams), i, i, vp, vp, vp, sz, P(CDecodeResult),
                                         P(CError)]),
         "prr_transform_blocks": (i, [vp, i, vp, vp, vp, sz]),

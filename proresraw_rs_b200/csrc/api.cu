@@ -538,13 +538,43 @@ int prr::build_develop_desc(const prr_header* h, const prr_params* params, int s
 
 namespace {
 
+uint32_t ceil_log2_u32(uint32_t v) {
+    uint32_t k = 0;
+    while (k < 32 && (uint64_t(1) << k) < v) k++;
+    return k;
+}
+
+prr_develop_config default_develop_config() {
+    prr_develop_config c{};
+    c.tile_w = 32;
+    c.tile_h = 32;
+    c.ctas_per_sm = 0;
+    return c;
+}
+
+// The launch shape for a frame: its bucket's config, the context's
+// occupancy cap (prr_develop_set_occupancy) over it when set.
+void apply_develop_config(const prr_ctx* c, const prr_develop_config& cfg, DevelopDesc* d) {
+    d->tile_w = cfg.tile_w;
+    d->tile_h = cfg.tile_h;
+    d->ctas_per_sm = c->develop_ctas ? c->develop_ctas : cfg.ctas_per_sm;
+}
+
 int develop_launch(prr_ctx* c, const prr_header* h, const prr_params* params, int stage,
-                   const uint16_t* dev_samples, int layout, float* r, float* g, float* b, size_t out_len) {
+                   const uint16_t* dev_samples, int layout, float* r, float* g, float* b, size_t out_len,
+                   const prr_develop_config* force = nullptr) {
     if (!c) return PRR_ERR_INVALID;
     DevelopDesc d{};
     PRR_TRY(build_develop_desc(h, params, stage, dev_samples, layout, r, g, b, out_len, &d));
     PRR_TRY(c->use_device());
-    d.ctas_per_sm = c->develop_ctas;
+    prr_develop_config cfg = default_develop_config();
+    if (force) {
+        cfg = *force;
+    } else {
+        const auto it = c->develop_cfgs.find(prr_develop_bucket(h->width, h->height));
+        if (it != c->develop_cfgs.end()) cfg = it->second;
+    }
+    apply_develop_config(c, cfg, &d);
     return c->cuda(launch_develop(d, c->stream));
 }
 
@@ -683,5 +713,80 @@ int prr_decode_components_events(prr_ctx* c, const uint8_t* packet, const uint32
 extern "C" int prr_develop_set_occupancy(prr_ctx* c, uint32_t ctas_per_sm) {
     if (!c || ctas_per_sm > 16) return PRR_ERR_INVALID;
     c->develop_ctas = ctas_per_sm;
+    return PRR_OK;
+}
+
+extern "C" uint32_t prr_develop_bucket(uint32_t width, uint32_t height) {
+    return (ceil_log2_u32(width) << 8) | ceil_log2_u32(height);
+}
+
+extern "C" int prr_develop_set_config(prr_ctx* c, uint32_t bucket, const prr_develop_config* cfg) {
+    if (!c || !cfg || !develop_shape_supported(cfg->tile_w, cfg->tile_h) || cfg->ctas_per_sm > 16)
+        return PRR_ERR_INVALID;
+    c->develop_cfgs[bucket] = *cfg;
+    return PRR_OK;
+}
+
+extern "C" int prr_develop_get_config(prr_ctx* c, uint32_t bucket, prr_develop_config* cfg) {
+    if (!c || !cfg) return PRR_ERR_INVALID;
+    const auto it = c->develop_cfgs.find(bucket);
+    *cfg = it != c->develop_cfgs.end() ? it->second : default_develop_config();
+    return PRR_OK;
+}
+
+extern "C" int prr_develop_tune(prr_ctx* c, const prr_header* h, const prr_params* params, int stage,
+                                const uint16_t* dev_samples, int layout, float* r, float* g, float* b,
+                                size_t out_len, uint32_t reps, prr_develop_config* best, float* best_ms) {
+    if (!c || !h) return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    reps = std::max(reps, 1u);
+    static const uint32_t shapes[][2] = {{32, 32}, {32, 16}, {64, 16}};
+    // CTAs per SM: as many as fit (0), and caps below that, down to half
+    // (a capped develop leaves room to kernels of other streams, and fewer
+    // resident CTAs wait less at their barriers).
+    std::vector<prr_develop_config> cands;
+    for (const auto& sh : shapes) {
+        const uint32_t threads = sh[0] * sh[1] / 4;
+        const uint32_t fit = std::max(1u, 1024u / threads);  // 64 registers a thread
+        for (uint32_t cap = 0; cap <= fit; cap = cap == 0 ? std::max(1u, fit / 2) : cap + 1) {
+            if (cap == fit) break;
+            prr_develop_config cfg{sh[0], sh[1], cap};
+            cands.push_back(cfg);
+        }
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = c->cuda(cudaEventCreate(&e0));
+    if (rc == PRR_OK) rc = c->cuda(cudaEventCreate(&e1));
+    prr_develop_config win = default_develop_config();
+    float win_ms = 1e30f;
+    for (size_t k = 0; rc == PRR_OK && k < cands.size(); k++) {
+        const prr_develop_config& cfg = cands[k];
+        const uint32_t saved = c->develop_ctas;
+        c->develop_ctas = 0;  // the candidate's own cap
+        std::vector<float> ms;
+        for (uint32_t i = 0; rc == PRR_OK && i <= reps; i++) {
+            rc = c->cuda(cudaEventRecord(e0, c->stream));
+            if (rc == PRR_OK) rc = develop_launch(c, h, params, stage, dev_samples, layout, r, g, b, out_len, &cfg);
+            if (rc == PRR_OK) rc = c->cuda(cudaEventRecord(e1, c->stream));
+            if (rc == PRR_OK) rc = c->cuda(cudaEventSynchronize(e1));
+            float t = 0.f;
+            if (rc == PRR_OK) rc = c->cuda(cudaEventElapsedTime(&t, e0, e1));
+            if (i > 0) ms.push_back(t);  // the first run is untimed
+        }
+        c->develop_ctas = saved;
+        if (rc != PRR_OK) break;
+        std::sort(ms.begin(), ms.end());
+        const float med = ms[ms.size() / 2];
+        if (med < win_ms) {
+            win_ms = med;
+            win = cfg;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    PRR_TRY(rc);
+    c->develop_cfgs[prr_develop_bucket(h->width, h->height)] = win;
+    if (best) *best = win;
+    if (best_ms) *best_ms = win_ms;
     return PRR_OK;
 }

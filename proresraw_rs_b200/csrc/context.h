@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -83,6 +84,7 @@ struct prr_ctx {
     HostBuf<uint64_t> lj_hoffsets;
     DevBuf<uint16_t> lin;
     uint32_t develop_ctas = 0;  // prr_develop_set_occupancy
+    std::map<uint32_t, prr_develop_config> develop_cfgs;  // per frame-size bucket (prr_develop_tune)
     prr::BatchState* batch = nullptr;
     prr::LearnedState* learned = nullptr;
     std::string last_error;

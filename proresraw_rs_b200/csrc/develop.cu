@@ -259,15 +259,30 @@ __device__ __forceinline__ float2 estimate2_x2(float2 xu, float2 xv, float2 gu, 
     return make_float2(okx ? r.x : mean_x.x, oky ? r.y : mean_x.y);
 }
 
-constexpr int TW = 32, TH = 32;           // output tile
-constexpr int NW = TW + 6, NH = TH + 6;   // normalized values, 3-sensel halo
-constexpr int GW = TW + 2, GH = TH + 2;   // green-pass region, 1-sensel halo
-constexpr int kDevThreads = 256;          // one thread per 2x2 quad of the tile
-
-// The tile's code values with the halo, as one TMA box: 38 rows of 48
-// sensels from x0 - 8 (the box's first column must sit on a 16-byte
-// boundary), of which columns 5 .. 42 are the 38 the tile reads.
-constexpr int kBoxW = 48, kBoxX = 5;
+// A tile shape of the develop: TW x TH output sensels (TW a power of two),
+// one thread per 2x2 quad. The shapes the autotuner chooses from are
+// instantiated below; 32x32 is the default and the only shape a tile mask
+// (the learned develop's fallback) addresses.
+template <int TW_, int TH_>
+struct Tile {
+    static constexpr int TW = TW_, TH = TH_;
+    static constexpr int NW = TW + 6, NH = TH + 6;  // normalized values, 3-sensel halo
+    static constexpr int GW = TW + 2, GH = TH + 2;  // green-pass region, 1-sensel halo
+    static constexpr int QW = TW / 2;               // quads per tile row
+    static constexpr int kThreads = (TW / 2) * (TH / 2);
+    // Resident CTAs per SM the registers are budgeted for (64 a thread).
+    static constexpr int kMinBlocks = 1024 / kThreads;
+    // The tile's code values with the halo, as one TMA box: NH rows of
+    // kBoxW sensels from x0 - 8 (the box's first column must sit on a
+    // 16-byte boundary), of which columns kBoxX .. kBoxX + NW - 1 are the
+    // ones the tile reads.
+    static constexpr int kBoxX = 5;
+    static constexpr int kBoxW = (kBoxX + NW + 7) / 8 * 8;
+    static_assert((TW & (TW - 1)) == 0 && TW >= 16 && TH % 2 == 0, "tile shape");
+};
+using Tile32x32 = Tile<32, 32>;
+using Tile32x16 = Tile<32, 16>;
+using Tile64x16 = Tile<64, 16>;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -298,7 +313,9 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint64_t limit_ns) {
     return false;
 }
 
+template <class T>
 struct DevShared {
+    static constexpr int NW = T::NW, NH = T::NH, GW = T::GW, GH = T::GH;
     float nrm[NH][NW];
     // Green-pass noise terms of every normalized value once clipped at its
     // own site's limit (1 at green sites, 1/gain at red and blue sites):
@@ -343,9 +360,10 @@ __device__ __forceinline__ void finish_x2(float2 r, float2 g, float2 b, const De
 // estimates (src/demosaic.rs:662-669) as the lanes of one pair, each green
 // site's horizontal and vertical estimates (src/demosaic.rs:670-680) as the
 // lanes of one pair. Returns per quad row the (r, g, b) pairs of its sites.
-template <int A>
-__device__ __forceinline__ void chroma_quad(const DevShared& S, int gyb, int gxb, bool red0, const DevelopDesc& d,
+template <class T, int A>
+__device__ __forceinline__ void chroma_quad(const DevShared<T>& S, int gyb, int gxb, bool red0, const DevelopDesc& d,
                                             float2 (&out)[2][3]) {
+    constexpr int GW = T::GW;
     // Region site of the quad offset (dy, dx).
     auto idx = [&](int dy, int dx) { return (gyb + dy) * GW + gxb + dx; };
     const float* rb = &S.rb[0][0];
@@ -417,10 +435,12 @@ __device__ __forceinline__ void chroma_quad(const DevShared& S, int gyb, int gxb
 // Four CTAs per SM (64 registers a thread): the kernel is bound by
 // instruction issue and loses more to three CTAs' fewer warps than it gains
 // from the registers it would spill less.
-template <bool PRE>
-__global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constant__ CUtensorMap codes_map,
-                                                         DevelopDesc d) {
-    __shared__ __align__(16) DevShared S;
+template <bool PRE, class T>
+__global__ void __launch_bounds__(T::kThreads, T::kMinBlocks) k_develop(const __grid_constant__ CUtensorMap codes_map,
+                                                                     DevelopDesc d) {
+    constexpr int TW = T::TW, TH = T::TH, NW = T::NW, NH = T::NH, GW = T::GW, GH = T::GH;
+    constexpr int kDevThreads = T::kThreads, kBoxW = T::kBoxW, kBoxX = T::kBoxX;
+    __shared__ __align__(16) DevShared<T> S;
     __shared__ __align__(128) uint16_t box[NH][kBoxW];
     __shared__ __align__(8) uint64_t box_bar;
     // Only the tiles a mask selects (the learned develop's fallback tiles).
@@ -668,7 +688,7 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
         // columns 2 qx + 1, 2 qx + 2): its red/blue pair, the heavy work,
         // one per thread.
         {
-            const int gy0 = 2 * (tid >> 4) + 1, gxq = 2 * (tid & 15) + 1;
+            const int gy0 = 2 * (tid / T::QW) + 1, gxq = 2 * (tid % T::QW) + 1;
             const int f0 = first_of(gy0);
             site_pair(true, gy0, gxq + f0, gxq + 1 - f0);
         }
@@ -717,7 +737,7 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
     }
     __syncthreads();
     // 3. Chroma (+ matrix) per quad.
-    const int qx = tid & 15, qy = tid >> 4;
+    const int qx = tid % T::QW, qy = tid / T::QW;
     const int xb = x0 + 2 * qx, yb = y0 + 2 * qy;
     if (xb >= w || yb >= h) return;
     if (!near_edge) {
@@ -725,9 +745,9 @@ __global__ void __launch_bounds__(kDevThreads, 4) k_develop(const __grid_constan
         const bool red0 = red_row == 0;
         float2 o2[2][3];
         if ((red0 ? red_col : 1 - red_col) == 0)
-            chroma_quad<0>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
+            chroma_quad<T, 0>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
         else
-            chroma_quad<1>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
+            chroma_quad<T, 1>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
         // The planes are written once and not read here again: streaming
         // stores (evict first) leave L2 to the next frame's decode beside.
 #pragma unroll
@@ -877,9 +897,9 @@ cudaError_t launch_linearize(const uint16_t* codes, uint32_t stride, int w, int 
 
 namespace {
 
-// Dynamic shared memory that caps k_develop<PRE> at `ctas` CTAs per SM
+// Dynamic shared memory that caps k_develop<PRE, T> at `ctas` CTAs per SM
 // (0: none), found with the occupancy calculator and kept per cap.
-template <bool PRE>
+template <bool PRE, class T>
 cudaError_t develop_reserve(uint32_t ctas, size_t* bytes) {
     *bytes = 0;
     if (ctas == 0) return cudaSuccess;
@@ -898,19 +918,19 @@ cudaError_t develop_reserve(uint32_t ctas, size_t* bytes) {
     cudaFuncAttributes fa;
     e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_develop<PRE>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_develop<PRE, T>);
     if (e != cudaSuccess) return e;
     const size_t fixed = fa.sharedSizeBytes;  // the kernel's static shared memory
     // A block's static plus dynamic shared memory above 48 KB needs the
     // opt-in limit.
-    e = cudaFuncSetAttribute(k_develop<PRE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_develop<PRE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(std::min<size_t>(size_t(per_block) - fixed, size_t(per_sm))));
     if (e != cudaSuccess) return e;
     const size_t step = 1024;
     size_t pad = 0;
     for (;;) {
         int n = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_develop<PRE>, kDevThreads, pad);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_develop<PRE, T>, T::kThreads, pad);
         if (e != cudaSuccess) return e;
         if (n <= int(ctas) || pad + fixed + step > size_t(per_block)) break;
         pad += step;
@@ -920,12 +940,9 @@ cudaError_t develop_reserve(uint32_t ctas, size_t* bytes) {
     return cudaSuccess;
 }
 
-}  // namespace
-
-cudaError_t launch_develop(const DevelopDesc& desc, cudaStream_t s) {
-    if (desc.w <= 0 || desc.h <= 0) return cudaSuccess;
-    DevelopDesc d = desc;
-    dim3 grid((d.w + TW - 1) / TW, (d.h + TH - 1) / TH);
+template <class T>
+cudaError_t launch_develop_shape(DevelopDesc d, cudaStream_t s) {
+    dim3 grid((d.w + T::TW - 1) / T::TW, (d.h + T::TH - 1) / T::TH);
     // The code values as a 2-D tensor (rows of the coded width, the
     // picture's height) for the TMA tile loads; a buffer that is not 16-byte
     // aligned, or a map the driver refuses, leaves every tile to the
@@ -933,21 +950,38 @@ cudaError_t launch_develop(const DevelopDesc& desc, cudaStream_t s) {
     alignas(64) CUtensorMap map;
     std::memset(&map, 0, sizeof(map));
     d.use_tma = 0;
-    if ((reinterpret_cast<uintptr_t>(d.codes) & 15) == 0 && (d.stride * 2) % 16 == 0 && d.w >= TW + 6 &&
-        d.h >= TH + 6)
-        d.use_tma = encode_u16_map_2d(&map, d.codes, d.stride, uint64_t(d.h), uint64_t(d.stride) * 2, kBoxW, NH) ==
-                    cudaSuccess;
+    if ((reinterpret_cast<uintptr_t>(d.codes) & 15) == 0 && (d.stride * 2) % 16 == 0 && d.w >= T::TW + 6 &&
+        d.h >= T::TH + 6)
+        d.use_tma = encode_u16_map_2d(&map, d.codes, d.stride, uint64_t(d.h), uint64_t(d.stride) * 2, T::kBoxW,
+                                      T::NH) == cudaSuccess;
     size_t pad = 0;
     cudaError_t e;
     if (d.w >= 4 && d.h >= 4) {
-        if ((e = develop_reserve<true>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
-        k_develop<true><<<grid, kDevThreads, pad, s>>>(map, d);
+        if ((e = develop_reserve<true, T>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
+        k_develop<true, T><<<grid, T::kThreads, pad, s>>>(map, d);
     } else {
-        if ((e = develop_reserve<false>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
-        k_develop<false><<<grid, kDevThreads, pad, s>>>(map, d);
+        if ((e = develop_reserve<false, T>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
+        k_develop<false, T><<<grid, T::kThreads, pad, s>>>(map, d);
     }
     count_launch();
     return cudaGetLastError();
+}
+
+}  // namespace
+
+bool develop_shape_supported(uint32_t tile_w, uint32_t tile_h) {
+    return (tile_w == 32 && (tile_h == 32 || tile_h == 16)) || (tile_w == 64 && tile_h == 16);
+}
+
+cudaError_t launch_develop(const DevelopDesc& d, cudaStream_t s) {
+    if (d.w <= 0 || d.h <= 0) return cudaSuccess;
+    const uint32_t tw = d.tile_w ? d.tile_w : 32, th = d.tile_h ? d.tile_h : 32;
+    // A tile mask addresses the 32x32 tile grid.
+    if (d.tile_mask && (tw != 32 || th != 32)) return cudaErrorInvalidValue;
+    if (tw == 32 && th == 32) return launch_develop_shape<Tile32x32>(d, s);
+    if (tw == 32 && th == 16) return launch_develop_shape<Tile32x16>(d, s);
+    if (tw == 64 && th == 16) return launch_develop_shape<Tile64x16>(d, s);
+    return cudaErrorInvalidValue;
 }
 
 }  // namespace prr

@@ -148,6 +148,8 @@ struct DevelopDesc {
     uint32_t ctas_per_sm;
     // Set by launch_develop: interior tiles load their code values by TMA.
     uint32_t use_tma;
+    // Output tile shape (0, 0: 32 x 32); see develop_shape_supported.
+    uint32_t tile_w, tile_h;
 };
 
 constexpr int kDevelopTile = 32;
@@ -164,6 +166,9 @@ cudaError_t launch_linearize(const uint16_t* codes, uint32_t stride, int w, int 
                              const uint32_t* c0, const uint32_t* delta, uint16_t* out,
                              cudaStream_t s);
 cudaError_t launch_develop(const DevelopDesc& d, cudaStream_t s);
+// The develop tile shapes launch_develop instantiates: 32x32 (default),
+// 32x16 and 64x16.
+bool develop_shape_supported(uint32_t tile_w, uint32_t tile_h);
 // learned.cu: a 2-D tensor map of 16-bit elements (cuTensorMapEncodeTiled
 // through the runtime's driver entry point).
 cudaError_t encode_u16_map_2d(CUtensorMap* map, const void* base, uint64_t width, uint64_t height,

@@ -76,3 +76,11 @@ def test_noalloc_refuses_device_ordinals_out_of_range_before_any_cuda_call():
         assert L.prr_decode_noalloc(device, None, C.byref(info), p, 0, p, p, p) == _lib.ERR_INVALID
     info.ntiles = _lib.NOALLOC_MAX_TILES + 1
     assert L.prr_decode_noalloc(0, None, C.byref(info), p, 0, p, p, p) == _lib.ERR_SCRATCH_LIMIT
+
+
+def test_develop_buckets_group_frame_sizes_by_power_of_two():
+    L = _lib.lib()
+    assert L.prr_develop_bucket(5760, 3040) == (13 << 8) | 12
+    assert L.prr_develop_bucket(4096, 2160) == (12 << 8) | 12
+    assert L.prr_develop_bucket(4097, 2048) == (13 << 8) | 11
+    assert L.prr_develop_set_config(None, 0, None) == _lib.ERR_INVALID
