@@ -594,6 +594,19 @@ int prr_transform_blocks(prr_ctx* ctx, int kind, const int16_t* dev_coefs, const
 int prr_decode_components(prr_ctx* ctx, const uint8_t* dev_packet, const uint32_t* dev_off,
                           const uint32_t* dev_len, size_t n, int log2_blocks, int log2_coefs,
                           int16_t* dev_coefs);
+/* The develop's paired division (fastdiv.cuh in the library's sources):
+ * q[i] = a[i] / b[i] rounded to nearest, two a thread as the develop runs
+ * it. It equals IEEE division for |a|, |b| in [2^-100, 2^100] and quotients
+ * in [2^-120, 2^120] (outside that range the develop does not use it).
+ * Device arrays; asynchronous. No counterpart in the crate. */
+int prr_div_rn_pairs(prr_ctx* ctx, const float* dev_a, const float* dev_b, float* dev_q, size_t n);
+/* Adds to *dev_mismatches (a device u64) the number of pairs (a, b), a over
+ * every significand in [1, 2), b over the significands [b_first, b_first +
+ * b_count) of [1, 2) (of 2^23), whose paired quotient differs from IEEE
+ * division, plus each b whose paired reciprocal does not scale exactly
+ * over the exponents [-100, 100]. b_first = 0, b_count = 2^23 checks all
+ * 2^46 pairs. Asynchronous. No counterpart in the crate. */
+int prr_div_rn_check(prr_ctx* ctx, uint32_t b_first, uint32_t b_count, uint64_t* dev_mismatches);
 /* The same streams through the frame decode's entropy decoder (the one the
  * full and reduced frame decodes and the batch decode run; the decoder
  * above is the one inside the fused transform kernels): each stream's

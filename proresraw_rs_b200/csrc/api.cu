@@ -696,6 +696,19 @@ int prr_decode_components(prr_ctx* c, const uint8_t* packet, const uint32_t* off
     return c->cuda(launch_decode_components(packet, off, len, n, log2_blocks, log2_coefs, coefs, c->stream));
 }
 
+int prr_div_rn_pairs(prr_ctx* c, const float* a, const float* b, float* q, size_t n) {
+    if (!c || (n && (!a || !b || !q))) return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    return c->cuda(launch_div_rn_pairs(a, b, q, n, c->stream));
+}
+
+int prr_div_rn_check(prr_ctx* c, uint32_t b_first, uint32_t b_count, uint64_t* dev_mismatches) {
+    if (!c || !dev_mismatches || b_first >= (1u << 23) || b_count > (1u << 23) - b_first) return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    return c->cuda(launch_div_rn_check(b_first, b_count, reinterpret_cast<unsigned long long*>(dev_mismatches),
+                                       c->stream));
+}
+
 int prr_decode_components_events(prr_ctx* c, const uint8_t* packet, const uint32_t* off, const uint32_t* len,
                                  size_t n, int log2_blocks, int log2_coefs, int staged, uint32_t* lists,
                                  int16_t* coefs, uint32_t* flags) {

@@ -24,6 +24,7 @@
 #include <cstring>
 
 #include "device_common.cuh"
+#include "fastdiv.cuh"
 #include "kernels.h"
 
 namespace prr {
@@ -154,8 +155,28 @@ __device__ __forceinline__ float2 variance2(float2 v, float off, const Noise& n)
     return add2(bc(n.c), make_float2(fmaxf(n.b, m.x), fmaxf(n.b, m.y)));
 }
 
+// The estimates' last quotient, weight = a / (b + a), of both lanes. Its
+// numerator a is at least three times the noise floor; its denominator
+// grows with the spread of the estimate's ratios and, for extreme
+// neighbourhoods, can leave the range the paired division is exact in, so
+// lanes whose denominator is above 2^60 take div.rn.
+template <bool FAST>
+__device__ __forceinline__ float2 weight_x2(float2 a, float2 den, bool okx, bool oky) {
+    float2 weight = a;
+    if (FAST && !((okx & !(den.x <= 0x1p60f)) | (oky & !(den.y <= 0x1p60f)))) {
+        weight = div_rn_x2(a, den);
+    } else {
+        if (okx) weight.x = dv(a.x, den.x);
+        if (oky) weight.y = dv(a.y, den.y);
+    }
+    return weight;
+}
+
 // estimate() of two sites, one a lane (src/demosaic.rs:572-604). A lane
-// whose test fails returns its mean; its divisions are skipped.
+// whose test fails returns its mean. FAST: the quotients by the paired
+// division (fastdiv.cuh), both lanes at once; else a failing lane's
+// divisions are skipped.
+template <bool FAST>
 __device__ __forceinline__ float2 estimate_x2(const float2* xx, const float2* gg, const float2* var_x,
                                               const float2* sx, const float2* sg, float2 cg, float2 cs) {
     const float2 q = bc(0.25f);
@@ -181,17 +202,25 @@ __device__ __forceinline__ float2 estimate_x2(const float2* xx, const float2* gg
         const float2 nlo = mul2(k1, sub2(xx[i], sx[i])), dlo = add2(sg[i], gg[i]);
         const float2 nmid = mul2(cg, xx[i]);
         const float2 nhi = mul2(k2, add2(sx[i], xx[i])), dhi = sub2(gg[i], sg[i]);
-        // A failing lane keeps its numerators (never used).
-        float2 lo = nlo, md = nmid, hi = nhi;
-        if (okx) {
-            lo.x = dv(nlo.x, dlo.x);
-            md.x = dv(nmid.x, gg[i].x);
-            hi.x = dv(nhi.x, dhi.x);
-        }
-        if (oky) {
-            lo.y = dv(nlo.y, dlo.y);
-            md.y = dv(nmid.y, gg[i].y);
-            hi.y = dv(nhi.y, dhi.y);
+        float2 lo, md, hi;
+        if (FAST) {
+            // Both lanes at once (a failing lane's quotients are never used).
+            lo = div_rn_x2(nlo, dlo);
+            md = div_rn_x2(nmid, gg[i]);
+            hi = div_rn_x2(nhi, dhi);
+        } else {
+            // A failing lane keeps its numerators (never used).
+            lo = nlo, md = nmid, hi = nhi;
+            if (okx) {
+                lo.x = dv(nlo.x, dlo.x);
+                md.x = dv(nmid.x, gg[i].x);
+                hi.x = dv(nhi.x, dhi.x);
+            }
+            if (oky) {
+                lo.y = dv(nlo.y, dlo.y);
+                md.y = dv(nmid.y, gg[i].y);
+                hi.y = dv(nhi.y, dhi.y);
+            }
         }
         mid[i] = md;
         ml[i] = sub2(md, lo);
@@ -203,14 +232,13 @@ __device__ __forceinline__ float2 estimate_x2(const float2* xx, const float2* gg
                  dm3 = sub2(mid[3], mean_mid);
     const float2 b = fma2(spread, bc(0.75f), dot4x2(dm0, dm1, dm2, dm3, dm0, dm1, dm2, dm3));
     const float2 den = add2(b, a);
-    float2 weight = a;
-    if (okx) weight.x = dv(a.x, den.x);
-    if (oky) weight.y = dv(a.y, den.y);
+    const float2 weight = weight_x2<FAST>(a, den, okx, oky);
     const float2 r = fma2(sub2(mean_mid, mean_x), weight, mean_x);
     return make_float2(okx ? r.x : mean_x.x, oky ? r.y : mean_x.y);
 }
 
 // estimate2() of two (u, v) neighbour pairs, one a lane.
+template <bool FAST>
 __device__ __forceinline__ float2 estimate2_x2(float2 xu, float2 xv, float2 gu, float2 gv, float2 vu, float2 vv,
                                                float2 su, float2 sv, float2 tu, float2 tv, float2 cg, float2 cs) {
     const float2 q = bc(0.25f);
@@ -229,7 +257,16 @@ __device__ __forceinline__ float2 estimate2_x2(float2 xu, float2 xv, float2 gu, 
     const float2 dhi_u = sub2(gu, tu), dhi_v = sub2(gv, tv);
     // A failing lane keeps its numerators (never used).
     float2 lo_u = nlo_u, lo_v = nlo_v, mid_u = nmid_u, mid_v = nmid_v, hi_u = nhi_u, hi_v = nhi_v;
-    if (okx) {
+    if (FAST) {
+        // Both lanes at once (a failing lane's quotients are never used).
+        lo_u = div_rn_x2(nlo_u, dlo_u);
+        lo_v = div_rn_x2(nlo_v, dlo_v);
+        mid_u = div_rn_x2(nmid_u, gu);
+        mid_v = div_rn_x2(nmid_v, gv);
+        hi_u = div_rn_x2(nhi_u, dhi_u);
+        hi_v = div_rn_x2(nhi_v, dhi_v);
+    }
+    if (!FAST && okx) {
         lo_u.x = dv(nlo_u.x, dlo_u.x);
         lo_v.x = dv(nlo_v.x, dlo_v.x);
         mid_u.x = dv(nmid_u.x, gu.x);
@@ -237,7 +274,7 @@ __device__ __forceinline__ float2 estimate2_x2(float2 xu, float2 xv, float2 gu, 
         hi_u.x = dv(nhi_u.x, dhi_u.x);
         hi_v.x = dv(nhi_v.x, dhi_v.x);
     }
-    if (oky) {
+    if (!FAST && oky) {
         lo_u.y = dv(nlo_u.y, dlo_u.y);
         lo_v.y = dv(nlo_v.y, dlo_v.y);
         mid_u.y = dv(nmid_u.y, gu.y);
@@ -252,9 +289,7 @@ __device__ __forceinline__ float2 estimate2_x2(float2 xu, float2 xv, float2 gu, 
     const float2 dm_u = sub2(mid_u, mean_mid), dm_v = sub2(mid_v, mean_mid);
     const float2 b = fma2(spread, bc(0.75f), fma2(dm_v, dm_v, fma2(dm_u, dm_u, fma2(dm_u, dm_u, mul2(dm_v, dm_v)))));
     const float2 den = add2(b, a);
-    float2 weight = a;
-    if (okx) weight.x = dv(a.x, den.x);
-    if (oky) weight.y = dv(a.y, den.y);
+    const float2 weight = weight_x2<FAST>(a, den, okx, oky);
     const float2 r = fma2(sub2(mean_mid, mean_x), weight, mean_x);
     return make_float2(okx ? r.x : mean_x.x, oky ? r.y : mean_x.y);
 }
@@ -360,7 +395,7 @@ __device__ __forceinline__ void finish_x2(float2 r, float2 g, float2 b, const De
 // estimates (src/demosaic.rs:662-669) as the lanes of one pair, each green
 // site's horizontal and vertical estimates (src/demosaic.rs:670-680) as the
 // lanes of one pair. Returns per quad row the (r, g, b) pairs of its sites.
-template <class T, int A>
+template <class T, int A, bool FAST>
 __device__ __forceinline__ void chroma_quad(const DevShared<T>& S, int gyb, int gxb, bool red0, const DevelopDesc& d,
                                             float2 (&out)[2][3]) {
     constexpr int GW = T::GW;
@@ -377,7 +412,7 @@ __device__ __forceinline__ void chroma_quad(const DevShared<T>& S, int gyb, int 
     const int qn[4] = {idx(0, -A), idx(2, -A), idx(0, 2 - A), idx(2, 2 - A)};
     // Two (u, v) neighbour pairs as lanes: lane x (ux, vx_), lane y (uy, vy).
     auto pair2 = [&](int ux, int vx_, int uy, int vy, float2 cg, float2 cs) {
-        return estimate2_x2(make_float2(rb[ux], rb[uy]), make_float2(rb[vx_], rb[vy]), make_float2(gr[ux], gr[uy]),
+        return estimate2_x2<FAST>(make_float2(rb[ux], rb[uy]), make_float2(rb[vx_], rb[vy]), make_float2(gr[ux], gr[uy]),
                             make_float2(gr[vx_], gr[vy]), make_float2(vx[ux], vx[uy]), make_float2(vx[vx_], vx[vy]),
                             make_float2(sx[ux], sx[uy]), make_float2(sx[vx_], sx[vy]), make_float2(sg[ux], sg[uy]),
                             make_float2(sg[vx_], sg[vy]), cg, cs);
@@ -405,7 +440,7 @@ __device__ __forceinline__ void chroma_quad(const DevShared<T>& S, int gyb, int 
     }
     const int ca = idx(0, A), cb = idx(1, 1 - A);
     const float gc_a = gr[ca], gc_b = gr[cb];
-    const float2 e = estimate_x2(X, G, V, SX, SG, make_float2(gc_a, gc_b), make_float2(sg[ca], sg[cb]));
+    const float2 e = estimate_x2<FAST>(X, G, V, SX, SG, make_float2(gc_a, gc_b), make_float2(sg[ca], sg[cb]));
     const float c_a = rb[ca], c_b = rb[cb];
     // Site (0, A) lies on the first row, (1, 1 - A) on the second; on a red
     // row r is the site's own value, or for a green site the horizontal
@@ -435,7 +470,7 @@ __device__ __forceinline__ void chroma_quad(const DevShared<T>& S, int gyb, int 
 // Four CTAs per SM (64 registers a thread): the kernel is bound by
 // instruction issue and loses more to three CTAs' fewer warps than it gains
 // from the registers it would spill less.
-template <bool PRE, class T>
+template <bool PRE, class T, bool FAST>
 __global__ void __launch_bounds__(T::kThreads, T::kMinBlocks) k_develop(const __grid_constant__ CUtensorMap codes_map,
                                                                      DevelopDesc d) {
     constexpr int TW = T::TW, TH = T::TH, NW = T::NW, NH = T::NH, GW = T::GW, GH = T::GH;
@@ -657,8 +692,16 @@ __global__ void __launch_bounds__(T::kThreads, T::kMinBlocks) k_develop(const __
                         const bool ally = (dd[0].y > sd[0].y) & (dd[1].y > sd[1].y) & (dd[2].y > sd[2].y) &
                                           (dd[3].y > sd[3].y);
                         const float2 den = mul2(t0, bc(2.0f));
-                        if (condx & anyx & allx) ratio.x = dv(t2.x, den.x);
-                        if (condy & anyy & ally) ratio.y = dv(t2.y, den.y);
+                        const bool px = condx & anyx & allx, py = condy & anyy & ally;
+                        if (FAST) {
+                            if (px | py) {
+                                const float2 q = div_rn_x2(t2, den);
+                                ratio = make_float2(px ? q.x : 0.0f, py ? q.y : 0.0f);
+                            }
+                        } else {
+                            if (px) ratio.x = dv(t2.x, den.x);
+                            if (py) ratio.y = dv(t2.y, den.y);
+                        }
                     }
                     g[dir] = mul2(mul2(sums01, bc(0.5f)), sub2(bc(1.0f), ratio));
                     const float2 e0 = sub2(dd[0], g[dir]), e1 = sub2(dd[1], g[dir]), e2 = sub2(dd[2], c),
@@ -669,7 +712,7 @@ __global__ void __launch_bounds__(T::kThreads, T::kMinBlocks) k_develop(const __
                 }
                 rbv = c;
                 const float2 num = mul2(sub2(g[0], g[1]), e[1]), den = add2(e[0], e[1]);
-                gv_out = add2(g[1], make_float2(dv(num.x, den.x), dv(num.y, den.y)));
+                gv_out = add2(g[1], FAST ? div_rn_x2(num, den) : make_float2(dv(num.x, den.x), dv(num.y, den.y)));
                 const float2 vxx = variance2(rbv, d.chroma_off, nz);
                 S.vx[gy0][gx0] = vxx.x;
                 S.vx[gy1][gx1] = vxx.y;
@@ -745,9 +788,9 @@ __global__ void __launch_bounds__(T::kThreads, T::kMinBlocks) k_develop(const __
         const bool red0 = red_row == 0;
         float2 o2[2][3];
         if ((red0 ? red_col : 1 - red_col) == 0)
-            chroma_quad<T, 0>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
+            chroma_quad<T, 0, FAST>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
         else
-            chroma_quad<T, 1>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
+            chroma_quad<T, 1, FAST>(S, 2 * qy + 1, 2 * qx + 1, red0, d, o2);
         // The planes are written once and not read here again: streaming
         // stores (evict first) leave L2 to the next frame's decode beside.
 #pragma unroll
@@ -879,6 +922,66 @@ __global__ void k_linearize(const uint16_t* __restrict__ codes, uint32_t stride,
     }
 }
 
+// Diagnostics of the paired division (fastdiv.cuh): quotients of arrays,
+// two a thread as the develop computes them; and a count of the pairs
+// (a, b), a over all 2^23 significands in [1, 2) and b over the
+// significands [b_first, b_first + b_count), whose paired quotient differs
+// from div.rn.f32 (one b per CTA), plus the b whose reciprocal does not
+// scale exactly over the exponents [-100, 100].
+__global__ void k_div_rn_pairs(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ q,
+                               size_t n) {
+    const size_t i = 2 * (size_t(blockIdx.x) * blockDim.x + threadIdx.x);
+    if (i >= n) return;
+    const bool two = i + 1 < n;
+    const float2 r = div_rn_x2(make_float2(a[i], two ? a[i + 1] : 1.0f), make_float2(b[i], two ? b[i + 1] : 1.0f));
+    q[i] = r.x;
+    if (two) q[i + 1] = r.y;
+}
+
+__global__ void __launch_bounds__(256) k_div_rn_check(uint32_t b_first, unsigned long long* mismatches) {
+    const uint32_t bb = 0x3F800000u | (b_first + blockIdx.x);
+    const float bf = __uint_as_float(bb);
+    unsigned long long bad = 0;
+    // The reciprocal scales exactly with b: 1/(b 2^k) = (1/b) 2^-k for k in
+    // [-100, 100], so the pairs of [1, 2) x [1, 2) stand for every exponent.
+    if (threadIdx.x <= 200) {
+        const int k = int(threadIdx.x) - 100;
+        const float bk = __uint_as_float(uint32_t(int32_t(bb) + k * (1 << 23)));
+        const float sk = __uint_as_float(uint32_t(127 - k) << 23);  // 2^-k
+        const float y = rcp_rn_x2(make_float2(bf, bf), make_float2(-bf, -bf)).x;
+        const float yk = rcp_rn_x2(make_float2(bk, bk), make_float2(-bk, -bk)).x;
+        bad += __float_as_uint(yk) != __float_as_uint(__fmul_rn(y, sk));
+    }
+    for (uint32_t m = threadIdx.x; m < (1u << 22); m += blockDim.x) {
+        const float a0 = __uint_as_float(0x3F800000u | (2 * m)), a1 = __uint_as_float(0x3F800000u | (2 * m + 1));
+        const float2 r = div_rn_x2(make_float2(a0, a1), make_float2(bf, bf));
+        bad += (__float_as_uint(r.x) != __float_as_uint(__fdiv_rn(a0, bf))) +
+               (__float_as_uint(r.y) != __float_as_uint(__fdiv_rn(a1, bf)));
+    }
+    if (bad) atomicAdd(mismatches, bad);
+}
+
+cudaError_t launch_div_rn_pairs(const float* a, const float* b, float* q, size_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const size_t threads = (n + 1) / 2;
+    k_div_rn_pairs<<<unsigned((threads + 255) / 256), 256, 0, s>>>(a, b, q, n);
+    count_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_div_rn_check(uint32_t b_first, uint32_t b_count, unsigned long long* mismatches,
+                                cudaStream_t s) {
+    if (b_first >= (1u << 23) || b_count > (1u << 23) - b_first) return cudaErrorInvalidValue;
+    // At most 4096 significands of b a launch (2^35 pairs).
+    for (uint32_t k = 0; k < b_count; k += 4096) {
+        k_div_rn_check<<<std::min(4096u, b_count - k), 256, 0, s>>>(b_first + k, mismatches);
+        count_launch();
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t launch_linearize(const uint16_t* codes, uint32_t stride, int w, int h, const uint32_t* c0,
                              const uint32_t* delta, uint16_t* out, cudaStream_t s) {
     const size_t chunks = size_t((w + 7) / 8) * h;
@@ -897,9 +1000,9 @@ cudaError_t launch_linearize(const uint16_t* codes, uint32_t stride, int w, int 
 
 namespace {
 
-// Dynamic shared memory that caps k_develop<PRE, T> at `ctas` CTAs per SM
-// (0: none), found with the occupancy calculator and kept per cap.
-template <bool PRE, class T>
+// Dynamic shared memory that caps k_develop<PRE, T, FAST> at `ctas` CTAs
+// per SM (0: none), found with the occupancy calculator and kept per cap.
+template <bool PRE, class T, bool FAST>
 cudaError_t develop_reserve(uint32_t ctas, size_t* bytes) {
     *bytes = 0;
     if (ctas == 0) return cudaSuccess;
@@ -918,19 +1021,19 @@ cudaError_t develop_reserve(uint32_t ctas, size_t* bytes) {
     cudaFuncAttributes fa;
     e = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_develop<PRE, T>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_develop<PRE, T, FAST>);
     if (e != cudaSuccess) return e;
     const size_t fixed = fa.sharedSizeBytes;  // the kernel's static shared memory
     // A block's static plus dynamic shared memory above 48 KB needs the
     // opt-in limit.
-    e = cudaFuncSetAttribute(k_develop<PRE, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_develop<PRE, T, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(std::min<size_t>(size_t(per_block) - fixed, size_t(per_sm))));
     if (e != cudaSuccess) return e;
     const size_t step = 1024;
     size_t pad = 0;
     for (;;) {
         int n = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_develop<PRE, T>, T::kThreads, pad);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_develop<PRE, T, FAST>, T::kThreads, pad);
         if (e != cudaSuccess) return e;
         if (n <= int(ctas) || pad + fixed + step > size_t(per_block)) break;
         pad += step;
@@ -956,18 +1059,40 @@ cudaError_t launch_develop_shape(DevelopDesc d, cudaStream_t s) {
                                       T::NH) == cudaSuccess;
     size_t pad = 0;
     cudaError_t e;
-    if (d.w >= 4 && d.h >= 4) {
-        if ((e = develop_reserve<true, T>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
-        k_develop<true, T><<<grid, T::kThreads, pad, s>>>(map, d);
+    if (d.w >= 4 && d.h >= 4 && develop_fast_division_ok(d)) {
+        if ((e = develop_reserve<true, T, true>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
+        k_develop<true, T, true><<<grid, T::kThreads, pad, s>>>(map, d);
+    } else if (d.w >= 4 && d.h >= 4) {
+        if ((e = develop_reserve<true, T, false>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
+        k_develop<true, T, false><<<grid, T::kThreads, pad, s>>>(map, d);
     } else {
-        if ((e = develop_reserve<false, T>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
-        k_develop<false, T><<<grid, T::kThreads, pad, s>>>(map, d);
+        if ((e = develop_reserve<false, T, false>(d.ctas_per_sm, &pad)) != cudaSuccess) return e;
+        k_develop<false, T, false><<<grid, T::kThreads, pad, s>>>(map, d);
     }
     count_launch();
     return cudaGetLastError();
 }
 
 }  // namespace
+
+// The paired division (fastdiv.cuh) is exact for operands inside [2^-100,
+// 2^100] and quotients inside [2^-120, 2^120]. Under these parameter bounds
+// every quotient of the green and chroma passes of interior tiles is inside
+// (the estimates' weight is also checked per site): the noise floor c
+// bounds every noise deviation below by sqrt(c) >= 2^-20, so every divisor
+// and numerator the passes form once their tests pass is at least
+// (2^-20 * 2^-24)^2; normalized values are at most 65535 * one_over_range
+// <= 65535, green estimates at most 1.5 times that, variances at most c +
+// max(b, a (off + v)^2) <= 2^43. DemosaicParams::new and
+// ::with_white_balance always give such parameters (c = 64/3 / range^2 >=
+// 2^-28 for range <= 65535; a <= 140; b < 1); other parameters take div.rn
+// throughout.
+bool develop_fast_division_ok(const DevelopDesc& d) {
+    auto in = [](float v, float lo, float hi) { return v >= lo && v <= hi; };  // false for NaN
+    return in(d.noise[2], 0x1p-40f, 1.0f) && in(d.noise[0], 0.0f, 256.0f) && in(d.noise[1], 0.0f, 256.0f) &&
+           in(d.one_over_range, 0x1p-17f, 1.0f) && in(d.green_off, -65536.0f, 65536.0f) &&
+           in(d.chroma_off, -65536.0f, 65536.0f);
+}
 
 bool develop_shape_supported(uint32_t tile_w, uint32_t tile_h) {
     return (tile_w == 32 && (tile_h == 32 || tile_h == 16)) || (tile_w == 64 && tile_h == 16);

@@ -169,6 +169,12 @@ cudaError_t launch_develop(const DevelopDesc& d, cudaStream_t s);
 // The develop tile shapes launch_develop instantiates: 32x32 (default),
 // 32x16 and 64x16.
 bool develop_shape_supported(uint32_t tile_w, uint32_t tile_h);
+// Whether the develop's parameters keep every quotient of its green and
+// chroma passes in the range of the paired division (fastdiv.cuh).
+bool develop_fast_division_ok(const DevelopDesc& d);
+cudaError_t launch_div_rn_pairs(const float* a, const float* b, float* q, size_t n, cudaStream_t s);
+cudaError_t launch_div_rn_check(uint32_t b_first, uint32_t b_count, unsigned long long* mismatches,
+                                cudaStream_t s);
 // learned.cu: a 2-D tensor map of 16-bit elements (cuTensorMapEncodeTiled
 // through the runtime's driver entry point).
 cudaError_t encode_u16_map_2d(CUtensorMap* map, const void* base, uint64_t width, uint64_t height,
