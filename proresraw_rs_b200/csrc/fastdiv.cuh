@@ -29,28 +29,64 @@
 
 namespace prr {
 
+// The packed operations are written as PTX with an explicit .rn rounding
+// modifier. An explicit modifier makes the code generator treat each one
+// as an IEEE operation of its own: it may not fuse or reorder it with the
+// operations around it, so the quotient is exactly the one the steps above
+// define, wherever it is inlined.
+namespace fastdiv_detail {
+__device__ __forceinline__ unsigned long long pack(float2 v) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+    return r;
+}
+__device__ __forceinline__ float2 unpack(unsigned long long r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ unsigned long long fma_rn(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+    unsigned long long r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ unsigned long long mul_rn(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
 __device__ __forceinline__ float rcp_approx(float b) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
     return r;
 }
+}  // namespace fastdiv_detail
 
-// RN(1/b) for both lanes (b inside the range above; nb = -b).
-__device__ __forceinline__ float2 rcp_rn_x2(float2 b, float2 nb) {
-    const float2 y0 = make_float2(rcp_approx(b.x), rcp_approx(b.y));
-    const float2 e = __ffma2_rn(nb, y0, make_float2(1.0f, 1.0f));
-    return __ffma2_rn(y0, e, y0);
+// RN(1/b) for both lanes, b inside the range above (packed; nb = -b).
+__device__ __forceinline__ unsigned long long rcp_rn_x2_packed(float2 b, unsigned long long nb) {
+    using namespace fastdiv_detail;
+    const unsigned long long y0 = pack(make_float2(rcp_approx(b.x), rcp_approx(b.y)));
+    const unsigned long long e = fma_rn(nb, y0, pack(make_float2(1.0f, 1.0f)));
+    return fma_rn(y0, e, y0);
+}
+
+__device__ __forceinline__ float2 rcp_rn_x2(float2 b) {
+    using namespace fastdiv_detail;
+    return unpack(rcp_rn_x2_packed(b, pack(make_float2(-b.x, -b.y))));
 }
 
 // RN(a/b) for both lanes (operands inside the range above).
 __device__ __forceinline__ float2 div_rn_x2(float2 a, float2 b) {
-    const float2 nb = __fmul2_rn(b, make_float2(-1.0f, -1.0f));
-    const float2 y = rcp_rn_x2(b, nb);
-    const float2 q0 = __fmul2_rn(a, y);
-    const float2 r0 = __ffma2_rn(nb, q0, a);
-    const float2 q1 = __ffma2_rn(r0, y, q0);
-    const float2 r1 = __ffma2_rn(nb, q1, a);
-    return __ffma2_rn(r1, y, q1);
+    using namespace fastdiv_detail;
+    const unsigned long long pa = pack(a);
+    const unsigned long long nb = pack(make_float2(-b.x, -b.y));
+    const unsigned long long y = rcp_rn_x2_packed(b, nb);
+    const unsigned long long q0 = mul_rn(pa, y);
+    const unsigned long long r0 = fma_rn(nb, q0, pa);
+    const unsigned long long q1 = fma_rn(r0, y, q0);
+    const unsigned long long r1 = fma_rn(nb, q1, pa);
+    return unpack(fma_rn(r1, y, q1));
 }
 
 }  // namespace prr
