@@ -248,10 +248,12 @@ typedef struct prr_job {
 /* Launch shape of the batch kernel, per bucket of batches. */
 typedef struct prr_batch_config {
     uint32_t ctas_per_sm;  /* persistent CTAs per SM; 0: as many as fit */
-    uint32_t stage_bytes;  /* packet bytes a 128-tile entropy item stages in shared memory:
+    uint32_t stage_bytes;  /* packet bytes an entropy item stages in shared memory:
                               a multiple of 16, at most 98304 */
     uint32_t use_graph;    /* replay a CUDA graph captured for the bucket */
-    uint32_t pad;
+    uint32_t streams_per_thread; /* component streams each of a CTA's 256 threads decodes in an
+                                    entropy item: 1, 2 or 4 (items of 64, 128 or 256 tiles);
+                                    0: 2 */
 } prr_batch_config;
 
 /* Parse the jobs' packets, upload them and enqueue the batch on the

@@ -673,17 +673,23 @@ class BatchJob:
 
 @dataclasses.dataclass
 class BatchConfig:
-    """Launch shape of the batch kernel for one bucket of batches."""
+    """Launch shape of the batch kernel for one bucket of batches: CTAs per
+    SM, packet bytes an entropy item stages, graph replay, and the
+    component streams each thread decodes in an entropy item (1, 2 or 4:
+    items of 64, 128 or 256 tiles, 256 threads a CTA)."""
     ctas_per_sm: int = 0  # 0: as many as fit
     stage_bytes: int = 32 * 1024
     use_graph: bool = True
+    streams_per_thread: int = 2
 
     def _c(self) -> _lib.CBatchConfig:
-        return _lib.CBatchConfig(self.ctas_per_sm, self.stage_bytes, 1 if self.use_graph else 0, 0)
+        return _lib.CBatchConfig(self.ctas_per_sm, self.stage_bytes, 1 if self.use_graph else 0,
+                                 self.streams_per_thread)
 
     @staticmethod
     def _from_c(c: _lib.CBatchConfig) -> "BatchConfig":
-        return BatchConfig(int(c.ctas_per_sm), int(c.stage_bytes), bool(c.use_graph))
+        return BatchConfig(int(c.ctas_per_sm), int(c.stage_bytes), bool(c.use_graph),
+                           int(c.streams_per_thread) or 2)
 
 
 class BatchDecoder:

@@ -146,7 +146,7 @@ class CBatchConfig(C.Structure):
         ("ctas_per_sm", C.c_uint32),
         ("stage_bytes", C.c_uint32),
         ("use_graph", C.c_uint32),
-        ("pad", C.c_uint32),
+        ("streams_per_thread", C.c_uint32),
     ]
 
 

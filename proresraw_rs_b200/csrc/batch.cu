@@ -208,7 +208,6 @@ Totals plan_batch(prr_job* jobs, size_t n, std::vector<FramePlan>& plan) {
         f.pairs_off = t.pairs;
         t.pairs += up64((size_t(f.info.tile_rows) * columns * 4) << f.lc);
         t.tiles += ntiles;
-        t.ent_items += (ntiles + kBatchTilesPerChunk - 1) / kBatchTilesPerChunk;
         t.seg_items += f.info.tile_rows * ((columns + 15) / 16);
         plan.push_back(f);
     }
@@ -224,14 +223,20 @@ prr_batch_config default_config() {
     c.ctas_per_sm = 0;
     c.stage_bytes = 32 * 1024;
     c.use_graph = 1;
+    c.streams_per_thread = 2;
     return c;
 }
 
 int check_config(const prr_batch_config& c) {
     if (c.stage_bytes == 0 || c.stage_bytes > kBatchMaxStageBytes || (c.stage_bytes & 15) != 0)
         return PRR_ERR_INVALID;
+    if (c.streams_per_thread != 0 && c.streams_per_thread != 1 && c.streams_per_thread != 2 &&
+        c.streams_per_thread != 4)
+        return PRR_ERR_INVALID;
     return PRR_OK;
 }
+
+uint32_t streams_per_thread_of(const prr_batch_config& c) { return c.streams_per_thread ? c.streams_per_thread : 2; }
 
 // The jobs' packets into the pinned staging buffer at their planned
 // offsets. A large batch is copied by several host threads, each taking
@@ -336,6 +341,11 @@ int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force, c
     Bucket& bk = B->buckets[key];
     const prr_batch_config cfg = force ? *force : (bk.has_cfg ? bk.cfg : default_config());
     PRR_TRY(check_config(cfg));
+    // Entropy items of the launch shape: tiles_per_item tiles each.
+    const uint32_t spt = streams_per_thread_of(cfg), tiles_per_item = batch_tiles_per_item(spt);
+    t.ent_items = 0;
+    for (const FramePlan& f : B->plan) t.ent_items += (f.info.ntiles + tiles_per_item - 1) / tiles_per_item;
+    if (t.ent_items + uint64_t(t.seg_items) > 0xFFFFFFF0ull) return PRR_ERR_INVALID;
     // Frames rounded up to a power of two: batches of one bucket share the
     // tile-index grid (and so the graph).
     const uint32_t grid_frames = 1u << ceil_log2(nf);
@@ -369,7 +379,8 @@ int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force, c
     hh->seg_items = t.seg_items;
     hh->wait_limit_us = B->wait_limit_us;
     hh->drop_item = B->drop_item;
-    hh->pad[0] = hh->pad[1] = hh->pad[2] = 0;
+    hh->streams_per_thread = spt;
+    hh->pad[0] = hh->pad[1] = 0;
     uint32_t ent = 0, seg = 0;
     for (size_t i = 0; i < nf; i++) {
         const FramePlan& f = B->plan[i];
@@ -391,7 +402,7 @@ int submit(prr_ctx* c, prr_job* jobs, size_t n, const prr_batch_config* force, c
         F.lc = f.lc;
         F.ent_begin = ent;
         F.seg_begin = seg;
-        ent += (ntiles + kBatchTilesPerChunk - 1) / kBatchTilesPerChunk;
+        ent += (ntiles + tiles_per_item - 1) / tiles_per_item;
         seg += f.info.tile_rows * F.d.segs_per_row;
     }
     if (!staged) stage_packets(B->hpackets.p, jobs, B->plan, t.packet_bytes);
@@ -557,6 +568,8 @@ int prr_batch_tune(prr_ctx* c, prr_job* jobs, size_t n, uint32_t reps, prr_batch
     prr_batch_config win = default_config();
     float win_ms = 1e30f;
     static const uint32_t stages[] = {16 * 1024, 32 * 1024, 48 * 1024, 64 * 1024, 96 * 1024};
+    static const uint32_t spts[] = {1, 2, 4};
+    for (uint32_t spt : spts)
     for (uint32_t stage : stages) {
         int max_per_sm = 0;
         PRR_TRY(c->cuda(batch_max_ctas_per_sm(stage, &max_per_sm)));
@@ -565,6 +578,7 @@ int prr_batch_tune(prr_ctx* c, prr_job* jobs, size_t n, uint32_t reps, prr_batch
             cfg.ctas_per_sm = uint32_t(per_sm);
             cfg.stage_bytes = stage;
             cfg.use_graph = 1;
+            cfg.streams_per_thread = spt;
             std::vector<float> ms;
             // One untimed run captures the graph.
             for (uint32_t r = 0; r <= reps; r++) {

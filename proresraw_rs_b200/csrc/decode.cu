@@ -1112,17 +1112,18 @@ __device__ __forceinline__ uint32_t batch_frame_of(const BatchDesc& b, uint32_t 
 
 // The batch kernel's work items as separate functions, so that each gets
 // the registers it needs on its own instead of the sum of all of them.
-// An entropy item of the batch kernel: the 2 x blockDim.x streams of
-// kBatchTilesPerChunk tiles. The item's packet span is staged when it fits;
-// the streams are sorted by byte length (bitonic, two keys a thread) and
-// thread i decodes the i-th shortest and the i-th longest, so every lane
+// An entropy item of the batch kernel: the S x blockDim.x streams of
+// S x blockDim.x / 4 consecutive tiles (S = streams per thread, 1, 2 or 4).
+// The item's packet span is staged when it fits; the streams are sorted by
+// byte length (bitonic) and the sorted list is cut into pairs of the i-th
+// shortest and i-th longest, which the threads take in turn, so every lane
 // has about the same number of symbols to decode and the CTA's warps reach
 // the item's closing barrier together.
 template <uint32_t LC>
 __device__ __noinline__ void batch_entropy(const EntropyTables& T, uint32_t* stage, uint32_t stage_bytes,
                                            const FrameDesc& d, int greens, const uint32_t* tile_off,
-                                           prr_dev_status* st, uint32_t item, uint32_t* keys) {
-    const uint32_t n = 2 * blockDim.x;  // streams of the item (a power of two, at most 1024)
+                                           prr_dev_status* st, uint32_t item, uint32_t* keys, uint32_t spt) {
+    const uint32_t n = spt * blockDim.x;  // streams of the item (a power of two, at most 1024)
     const uint32_t g0 = item * n;
     const uint32_t t0 = g0 / 4;
     const uint32_t t1 = min(t0 + n / 4, d.ntiles);
@@ -1158,11 +1159,14 @@ __device__ __noinline__ void batch_entropy(const EntropyTables& T, uint32_t* sta
             __syncthreads();
         }
     }
+    // Sorted positions of this thread's streams: one (S = 1), or the pairs
+    // (k, n - 1 - k) for k = i, i + blockDim.x, ...
     const uint32_t i = threadIdx.x;
-    const uint32_t mine[2] = {keys[i] & 1023, keys[n - 1 - i] & 1023};
 #pragma unroll 1
-    for (int q = 0; q < 2; q++) {
-        const StreamJob jb = stream_job<LC>(d, greens, tile_off, g0 + mine[q]);
+    for (uint32_t q = 0; q < spt; q++) {
+        const uint32_t k = i + (q >> 1) * blockDim.x;
+        const uint32_t pos = spt == 1 ? i : ((q & 1) ? n - 1 - k : k);
+        const StreamJob jb = stream_job<LC>(d, greens, tile_off, g0 + (keys[pos] & 1023));
         if (!jb.valid) continue;
         uint32_t* list = d.pairs + stream_list_base(d, jb.trow, jb.x, jb.log2, jb.s, LC);
         bool revisited = false, ok = true;
@@ -1198,7 +1202,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
     __shared__ EntropyTables T;
     __shared__ FrameDesc fd;
     __shared__ uint32_t s_item, s_frame, s_epoch, s_ok;
-    __shared__ uint32_t keys[2 * kBatchThreads];  // the entropy items' stream order
+    __shared__ uint32_t keys[kBatchMaxStreamsPerThread * kBatchThreads];  // the entropy items' stream order
     const uint32_t tid = threadIdx.x;
     load_tables(&S.T);
     if (tid == 0) s_epoch = b.q->epoch;
@@ -1207,6 +1211,9 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
     const uint32_t nframes = b.hdr->nframes, ent_items = b.hdr->ent_items;
     const uint32_t total = ent_items + b.hdr->seg_items;
     const uint32_t drop_item = b.hdr->drop_item;
+    const uint32_t spt = (b.hdr->streams_per_thread == 1 || b.hdr->streams_per_thread == 4) ? b.hdr->streams_per_thread
+                                                                                          : 2u;
+    const uint32_t tiles_per_item = batch_tiles_per_item(spt);
     const uint64_t wait_ns = b.hdr->wait_limit_us ? uint64_t(b.hdr->wait_limit_us) * 1000u : kChunkWaitNs;
     for (;;) {
         __syncthreads();  // the previous item's shared memory is no longer read
@@ -1233,11 +1240,11 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
             __syncthreads();
             const uint32_t chunk = item - F.ent_begin;
             if (lc == 6)
-                batch_entropy<6>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk, keys);
+                batch_entropy<6>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk, keys, spt);
             else if (lc == 4)
-                batch_entropy<4>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk, keys);
+                batch_entropy<4>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk, keys, spt);
             else
-                batch_entropy<2>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk, keys);
+                batch_entropy<2>(T, stage, b.stage_bytes, fd, greens, F.tile_off, F.st, chunk, keys, spt);
             __syncthreads();
             if (tid == 0) {
                 __threadfence();
@@ -1256,7 +1263,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_decode(BatchDesc b) 
             const uint32_t first = trow * F.d.tiles_per_row + j0;
             const uint32_t last = trow * F.d.tiles_per_row + min(j0 + 15, F.d.tiles_per_row - 1);
             bool ok = true;
-            for (uint32_t c = first / kBatchTilesPerChunk; ok && c <= last / kBatchTilesPerChunk; c++)
+            for (uint32_t c = first / tiles_per_item; ok && c <= last / tiles_per_item; c++)
                 ok = wait_flag(b.flags + F.ent_begin + c, s_epoch, wait_ns);
             if (!ok) {
                 atomicOr(&b.q->error, 1u);

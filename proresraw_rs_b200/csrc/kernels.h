@@ -87,7 +87,8 @@ struct BatchHeader {
     uint32_t seg_items;      // segments of all frames
     uint32_t wait_limit_us;  // a segment's wait for a chunk flag (0: kChunkWaitNs)
     uint32_t drop_item;      // a chunk claimed but never decoded nor flagged (tests), or NO_TILE
-    uint32_t pad[3];
+    uint32_t streams_per_thread;  // of an entropy item: 1, 2 or 4 (tiles per item: 64 x it)
+    uint32_t pad[2];
 };
 
 struct BatchDesc {
@@ -99,8 +100,12 @@ struct BatchDesc {
 };
 
 constexpr uint32_t kBatchThreads = 256;
-// Tiles of an entropy item: two streams a thread (four streams a tile).
-constexpr uint32_t kBatchTilesPerChunk = kBatchThreads / 2;
+// Tiles of an entropy item: streams_per_thread x kBatchThreads streams,
+// four a tile.
+constexpr uint32_t kBatchMaxStreamsPerThread = 4;
+__host__ __device__ constexpr uint32_t batch_tiles_per_item(uint32_t streams_per_thread) {
+    return streams_per_thread * kBatchThreads / 4;
+}
 constexpr uint32_t kBatchMaxStageBytes = 96 * 1024;
 // Dynamic shared memory of the batch kernel for a packet stage of
 // stage_bytes (<= kBatchMaxStageBytes), and the CTAs per SM that fit.

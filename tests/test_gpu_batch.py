@@ -76,13 +76,23 @@ def test_corrupted_frames_keep_their_skipped_lists(corpus):
         assert_job(job, got, oracle_of(job))
 
 
-@pytest.mark.parametrize("stage,per_sm,graph", [(16384, 1, True), (32768, 0, False), (65536, 2, True),
-                                                (98304, 1, True)])
-def test_every_launch_shape_gives_the_same_frames(corpus, stage, per_sm, graph):
+@pytest.mark.parametrize("stage,per_sm,graph,spt", [(16384, 1, True, 2), (32768, 0, False, 2), (65536, 2, True, 2),
+                                                    (98304, 1, True, 2), (16384, 0, True, 1), (32768, 3, True, 1),
+                                                    (32768, 0, True, 4), (98304, 2, False, 4)])
+def test_every_launch_shape_gives_the_same_frames(corpus, stage, per_sm, graph, spt):
+    # Streams per thread of an entropy item (1, 2, 4: items of 64, 128 or
+    # 256 tiles) change which CTA decodes which stream and which chunk a
+    # segment waits for; every frame stays the oracle's.
     dec = P.BatchDecoder()
     jobs = jobs_of(corpus)
-    dec.set_config(dec.bucket(jobs), P.BatchConfig(per_sm, stage, graph))
+    dec.set_config(dec.bucket(jobs), P.BatchConfig(per_sm, stage, graph, spt))
     run_and_check(dec, jobs)
+
+
+def test_a_launch_shape_with_other_streams_per_thread_is_refused():
+    with pytest.raises(P.Error) as e:
+        P.BatchDecoder().set_config(0, P.BatchConfig(0, 32768, True, 3))
+    assert e.value.code == P._lib.ERR_INVALID
 
 
 def test_graph_replay_reads_each_new_batch(corpus):
@@ -134,7 +144,7 @@ def test_autotuner_picks_a_config_and_frames_stay_exact(corpus):
     dec = P.BatchDecoder()
     jobs = jobs_of(corpus[:12])
     cfg, ms = dec.tune(jobs, reps=1)
-    assert ms > 0 and cfg.stage_bytes % 16 == 0 and cfg.ctas_per_sm >= 1
+    assert ms > 0 and cfg.stage_bytes % 16 == 0 and cfg.ctas_per_sm >= 1 and cfg.streams_per_thread in (1, 2, 4)
     assert dec.get_config(dec.bucket(jobs)) == cfg
     run_and_check(dec, jobs)
 
