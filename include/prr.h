@@ -609,6 +609,12 @@ int prr_div_rn_pairs(prr_ctx* ctx, const float* dev_a, const float* dev_b, float
  * over the exponents [-100, 100]. b_first = 0, b_count = 2^23 checks all
  * 2^46 pairs. Asynchronous. No counterpart in the crate. */
 int prr_div_rn_check(prr_ctx* ctx, uint32_t b_first, uint32_t b_count, uint64_t* dev_mismatches);
+/* The develop's paired square root: adds to *dev_mismatches the number of
+ * floats with exponent in [e_min, e_max] (every significand) whose paired
+ * square root differs from IEEE sqrt. It equals IEEE sqrt on [2^-60, 2^60],
+ * the range the develop uses it in. Asynchronous. No counterpart in the
+ * crate. */
+int prr_sqrt_rn_check(prr_ctx* ctx, int e_min, int e_max, uint64_t* dev_mismatches);
 /* The same streams through the frame decode's entropy decoder (the one the
  * full and reduced frame decodes and the batch decode run; the decoder
  * above is the one inside the fused transform kernels): each stream's

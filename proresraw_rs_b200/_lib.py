@@ -284,6 +284,7 @@ def lib():
         "prr_decode_components_events": (i, [vp, vp, vp, vp, sz, i, i, i, vp, vp, vp]),
         "prr_div_rn_pairs": (i, [vp, vp, vp, vp, sz]),
         "prr_div_rn_check": (i, [vp, C.c_uint32, C.c_uint32, vp]),
+        "prr_sqrt_rn_check": (i, [vp, i, i, vp]),
         "prr_decode_noalloc": (i, [i, vp, P(CFrameInfo), vp, i, vp, vp, vp]),
         "prr_batch_submit": (i, [vp, P(CJob), sz]),
         "prr_batch_wait": (i, [vp, C.c_uint32]),

@@ -702,6 +702,13 @@ int prr_div_rn_pairs(prr_ctx* c, const float* a, const float* b, float* q, size_
     return c->cuda(launch_div_rn_pairs(a, b, q, n, c->stream));
 }
 
+int prr_sqrt_rn_check(prr_ctx* c, int e_min, int e_max, uint64_t* dev_mismatches) {
+    if (!c || !dev_mismatches || e_min < -126 || e_max > 127 || e_min > e_max) return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    return c->cuda(launch_sqrt_rn_check(e_min, e_max, reinterpret_cast<unsigned long long*>(dev_mismatches),
+                                        c->stream));
+}
+
 int prr_div_rn_check(prr_ctx* c, uint32_t b_first, uint32_t b_count, uint64_t* dev_mismatches) {
     if (!c || !dev_mismatches || b_first >= (1u << 23) || b_count > (1u << 23) - b_first) return PRR_ERR_INVALID;
     PRR_TRY(c->use_device());

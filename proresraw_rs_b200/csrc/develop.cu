@@ -538,7 +538,7 @@ __global__ void __launch_bounds__(T::kThreads, T::kMinBlocks) k_develop(const __
             const float lima = (xa & 1) == rbc ? rlim : 1.0f, limb = (xb & 1) == rbc ? rlim : 1.0f;
             const float2 var = variance2(make_float2(fminf(v.x, lima), fminf(v.y, limb)), d.green_off, nz);
             *reinterpret_cast<float2*>(&S.gvar[ty][tx]) = var;
-            *reinterpret_cast<float2*>(&S.gsd[ty][tx]) = make_float2(rt(var.x), rt(var.y));
+            *reinterpret_cast<float2*>(&S.gsd[ty][tx]) = FAST ? sqrt_rn_x2(var) : make_float2(rt(var.x), rt(var.y));
         }
     }
     __syncthreads();
@@ -721,16 +721,18 @@ __global__ void __launch_bounds__(T::kThreads, T::kMinBlocks) k_develop(const __
                 const float2 vxx = variance2(rbv, d.chroma_off, nz);
                 S.vx[gy0][gx0] = vxx.x;
                 S.vx[gy1][gx1] = vxx.y;
-                S.sx[gy0][gx0] = rt(vxx.x);
-                S.sx[gy1][gx1] = rt(vxx.y);
+                const float2 sxx = FAST ? sqrt_rn_x2(vxx) : make_float2(rt(vxx.x), rt(vxx.y));
+                S.sx[gy0][gx0] = sxx.x;
+                S.sx[gy1][gx1] = sxx.y;
             }
             const float2 vg = variance2(gv_out, d.chroma_off, nz);
             S.rb[gy0][gx0] = rbv.x;
             S.rb[gy1][gx1] = rbv.y;
             S.gr[gy0][gx0] = gv_out.x;
             S.gr[gy1][gx1] = gv_out.y;
-            S.sg[gy0][gx0] = rt(vg.x);
-            S.sg[gy1][gx1] = rt(vg.y);
+            const float2 sgg = FAST ? sqrt_rn_x2(vg) : make_float2(rt(vg.x), rt(vg.y));
+            S.sg[gy0][gx0] = sgg.x;
+            S.sg[gy1][gx1] = sgg.y;
         };
         // Each thread's quad of the tile (region rows 2 qy + 1, 2 qy + 2,
         // columns 2 qx + 1, 2 qx + 2): its red/blue pair, the heavy work,
@@ -1025,6 +1027,28 @@ __global__ void __launch_bounds__(256) k_div_rn_check(uint32_t b_first, unsigned
     if (bad) atomicAdd(mismatches, bad);
 }
 
+// Every float with exponent in [e_min, e_max] (one exponent per CTA, the
+// significands over its threads, two a thread): count those whose paired
+// square root differs from sqrt.rn.f32.
+__global__ void __launch_bounds__(256) k_sqrt_rn_check(int e_min, unsigned long long* mismatches) {
+    const uint32_t ex = uint32_t(e_min + int(blockIdx.x) + 127) << 23;
+    unsigned long long bad = 0;
+    for (uint32_t m = blockIdx.y * blockDim.x + threadIdx.x; m < (1u << 22); m += gridDim.y * blockDim.x) {
+        const float x0 = __uint_as_float(ex | (2 * m)), x1 = __uint_as_float(ex | (2 * m + 1));
+        const float2 r = sqrt_rn_x2(make_float2(x0, x1));
+        bad += (__float_as_uint(r.x) != __float_as_uint(__fsqrt_rn(x0))) +
+               (__float_as_uint(r.y) != __float_as_uint(__fsqrt_rn(x1)));
+    }
+    if (bad) atomicAdd(mismatches, bad);
+}
+
+cudaError_t launch_sqrt_rn_check(int e_min, int e_max, unsigned long long* mismatches, cudaStream_t s) {
+    if (e_min < -126 || e_max > 127 || e_min > e_max) return cudaErrorInvalidValue;
+    k_sqrt_rn_check<<<dim3(unsigned(e_max - e_min + 1), 64), 256, 0, s>>>(e_min, mismatches);
+    count_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_div_rn_pairs(const float* a, const float* b, float* q, size_t n, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     const size_t threads = (n + 1) / 2;
@@ -1124,7 +1148,8 @@ cudaError_t launch_develop_shape(DevelopDesc d, cudaStream_t s) {
 }  // namespace
 
 // The paired division (fastdiv.cuh) is exact for operands inside [2^-100,
-// 2^100] and quotients inside [2^-120, 2^120]. Under these parameter bounds
+// 2^100] and quotients inside [2^-120, 2^120], the paired square root on
+// [2^-60, 2^60] (every variance lies in [c, 2^43]). Under these parameter bounds
 // every quotient of the green and chroma passes of interior tiles is inside
 // (the estimates' weight is also checked per site): the noise floor c
 // bounds every noise deviation below by sqrt(c) >= 2^-20, so every divisor

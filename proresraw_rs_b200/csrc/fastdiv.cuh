@@ -61,6 +61,11 @@ __device__ __forceinline__ float rcp_approx(float b) {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
     return r;
 }
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 }  // namespace fastdiv_detail
 
 // RN(1/b) for both lanes, b inside the range above (packed; nb = -b).
@@ -87,6 +92,27 @@ __device__ __forceinline__ float2 div_rn_x2(float2 a, float2 b) {
     const unsigned long long q1 = fma_rn(r0, y, q0);
     const unsigned long long r1 = fma_rn(nb, q1, pa);
     return unpack(fma_rn(r1, y, q1));
+}
+
+// RN(sqrt(x)) for both lanes, x in [2^-60, 2^60], by the same method
+// (Markstein): from y0 = approximate 1/sqrt(x), g = RN(x y0) ~ sqrt(x) and
+// h = y0 / 2 ~ 1/(2 sqrt(x)); one coupled Newton step r = 0.5 - g h,
+// g1 = g + g r, h1 = h + h r; then the residual correction
+// s = g1 + h1 (x - g1 g1). Every float of that range is checked against
+// sqrt.rn.f32 by the library's tests (prr_sqrt_rn_check).
+__device__ __forceinline__ float2 sqrt_rn_x2(float2 x) {
+    using namespace fastdiv_detail;
+    const unsigned long long px = pack(x);
+    const unsigned long long y0 = pack(make_float2(rsqrt_approx(x.x), rsqrt_approx(x.y)));
+    const unsigned long long g = mul_rn(px, y0);
+    const unsigned long long h = mul_rn(y0, pack(make_float2(0.5f, 0.5f)));
+    const unsigned long long ng = mul_rn(g, pack(make_float2(-1.0f, -1.0f)));
+    const unsigned long long r = fma_rn(ng, h, pack(make_float2(0.5f, 0.5f)));
+    const unsigned long long g1 = fma_rn(g, r, g);
+    const unsigned long long h1 = fma_rn(h, r, h);
+    const unsigned long long ng1 = mul_rn(g1, pack(make_float2(-1.0f, -1.0f)));
+    const unsigned long long d = fma_rn(ng1, g1, px);
+    return unpack(fma_rn(d, h1, g1));
 }
 
 }  // namespace prr

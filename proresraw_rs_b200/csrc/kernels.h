@@ -178,6 +178,7 @@ bool develop_shape_supported(uint32_t tile_w, uint32_t tile_h);
 // chroma passes in the range of the paired division (fastdiv.cuh).
 bool develop_fast_division_ok(const DevelopDesc& d);
 cudaError_t launch_div_rn_pairs(const float* a, const float* b, float* q, size_t n, cudaStream_t s);
+cudaError_t launch_sqrt_rn_check(int e_min, int e_max, unsigned long long* mismatches, cudaStream_t s);
 cudaError_t launch_div_rn_check(uint32_t b_first, uint32_t b_count, unsigned long long* mismatches,
                                 cudaStream_t s);
 // learned.cu: a 2-D tensor map of 16-bit elements (cuTensorMapEncodeTiled

@@ -1,10 +1,10 @@
-"""The develop's paired division (fastdiv.cuh): Markstein's method on f32x2
-pairs must give IEEE round-to-nearest division bit for bit wherever the
-develop uses it -- |a|, |b| in [2^-100, 2^100], quotients in [2^-120,
-2^120]. Exhaustively on the significands (every pair of [1, 2) x [1, 2),
-with the reciprocal's exact scaling over the exponents), then on random
-operands across the range and on edge operands, against numpy's IEEE
-division."""
+"""The develop's paired division and square root (fastdiv.cuh): Markstein's
+method on f32x2 pairs must give IEEE round-to-nearest results bit for bit
+wherever the develop uses it. Division (|a|, |b| in [2^-100, 2^100],
+quotients in [2^-120, 2^120]): every significand pair of [1, 2) x [1, 2)
+with the reciprocal's exact scaling over the exponents, random operands
+across the range and edge operands, against numpy's IEEE division. Square
+root: every float of [2^-60, 2^61) against sqrt.rn."""
 
 import numpy as np
 import pytest
@@ -62,3 +62,14 @@ def test_edge_operands():
     a, b = a[keep], b[keep]
     got = pairs_dev(a, b)
     assert np.array_equal(got.view(np.uint32), (a / b).view(np.uint32))
+
+
+def test_every_float_in_the_develops_range_has_the_ieee_square_root():
+    # The paired square root (fastdiv.cuh) against sqrt.rn on every float of
+    # [2^-60, 2^61), the range the develop's variances lie in with margin.
+    import torch
+
+    bad = torch.zeros(1, dtype=torch.int64, device="cuda")
+    assert _lib.lib().prr_sqrt_rn_check(P.context(), -60, 60, bad.data_ptr()) == 0
+    torch.cuda.synchronize()
+    assert int(bad.item()) == 0
