@@ -78,3 +78,27 @@ def test_unsupported_shapes_are_refused():
     with pytest.raises(P.Error) as e:
         P.develop_set_config(P.develop_bucket(64, 64), P.DevelopConfig(16, 16, 0))
     assert e.value.code == _lib.ERR_INVALID
+
+
+@pytest.mark.parametrize("noise", [(0.0, 0.0, 1e-14), (3e-4, 1e-7, 2e-6), (1000.0, 0.0, 1e-6)],
+                         ids=["below-the-floor", "ordinary", "large-slope"])
+def test_parameters_outside_the_paired_division_range_take_ieee_division(noise):
+    # Parameters a caller sets by hand can leave the range in which the
+    # develop's paired division and square root are exact (a noise floor
+    # below 2^-40, a slope above 256): the develop then divides and takes
+    # roots with div.rn / sqrt.rn throughout. Both paths must be the
+    # oracle's, on interior and edge tiles, with these parameters.
+    import dataclasses
+
+    pkt = frame(700, 300, 0, seed=9)
+    o = O.decode_frame(pkt)
+    g = P.decode_frame(pkt)
+    prm = dataclasses.replace(P.DemosaicParams.new(g.header, g.quantizer()), noise=noise)
+    op = O.params_new(o.header, o.quantizer)
+    op.noise[:] = list(noise)
+    for stage in (0, 2):
+        want = O.develop(o, op, stage, planar=True)
+        got = P.develop_planar(g, prm, P.Stage(stage))
+        for c in range(3):
+            diff = np.count_nonzero(got.planes[c].cpu().numpy().view(np.uint32) != want[c].view(np.uint32))
+            assert diff == 0, f"stage {stage} plane {c}: {diff} differ"
