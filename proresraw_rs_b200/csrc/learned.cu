@@ -30,17 +30,16 @@
 // 8 x 16-byte core matrix of the tensor core's K-major operand layout);
 // head, gradients and colours f32 planar [image][C][H][W].
 //
-// Convolution on the tensor cores: one CTA computes a 32 x 16 pixel tile as
-// four M = 128 blocks (8 columns x 16 rows each). The input window (34 x 18
-// pixels, all chunks) and the layer's weights are staged in shared memory;
-// for each block, tap and 16-channel half, one thread issues
-// tcgen05.mma.cta_group::1.kind::f16 with M = 128, N = cout, K = 16: A is the
-// window shifted by the tap (start address moves by the tap's offset; the
-// next 8 rows of M are the next window row, the second K chunk the next
-// chunk plane), B the tap's weights [cout][16]. Accumulators live in tensor
-// memory (4 x cout columns); tcgen05.commit signals an mbarrier; each warp
-// reads its 32 lanes back with tcgen05.ld, adds the bias, applies ReLU and
-// stores bf16 chunks (or the f32 head).
+// Convolution on the tensor cores (k_sg_rows): a CTA streams the input rows
+// of a 128-pixel strip through shared memory; for each row, column offset
+// and 16-channel half, one thread issues tcgen05.mma.cta_group::1.kind::f16
+// with M = 128 (the strip's pixels: A is the row, its start address moved by
+// the column offset), K = 16 and N = 3 x cout: B stacks the three kernel
+// rows' weights, so one MMA adds the row's products to the three output rows
+// it touches, whose accumulators are consecutive slots of a ring in tensor
+// memory (the first MMA into a slot overwrites it). A finished output row
+// is read back with tcgen05.ld (a warp per 32 lanes), biased, rectified and
+// stored as bf16 chunks (or the f32 head, or the develop output).
 //
 // Backward (training only) runs on the CUDA cores in f32: the gradient of
 // each layer's input through the ReLU, and weight and bias gradients reduced
@@ -53,6 +52,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -81,31 +81,36 @@ __host__ __device__ constexpr size_t packed_off(int l) {  // bf16 elements
 constexpr size_t kParams = layer_off(kLayers);
 constexpr size_t kPacked = packed_off(kLayers);
 
-constexpr int TX = 32, TY = 16;          // output tile of a conv CTA
-constexpr int WY = TY + 2;              // input window rows
 constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
 
-// The window is staged as two overlapping halves of HX columns (window
-// columns 0-17 and 16-33): M blocks 0-1 read the first, 2-3 the second. A
-// half's row of one chunk is 18 x 16 = 288 contiguous bytes in the
-// activation tensor, so each half is one TMA box with long rows.
-constexpr int HX = 18;
+// Row-streaming convolution (k_sg_rows below): a CTA computes strips of RM
+// output pixels of a run of rows; an input row of a strip is RW pixels.
+constexpr int RM = 128, RW = RM + 2;
+constexpr int kRowSlots = 8;                 // accumulator ring in tensor memory, output rows
+constexpr int kRowPairs = kRowSlots / 2;     // ... as pairs of adjacent rows
+constexpr int kRowStages = 4;                // ring of shared-memory stages, two input rows each
+constexpr int kRowEpiWarps = 4 * kRowPairs;  // an epilogue group of four warps (128 lanes) per pair
+constexpr int kRowProducerWarp = kRowEpiWarps, kRowMmaWarp = kRowEpiWarps + 1;
+constexpr int kRowThreads = 32 * (kRowEpiWarps + 2);
+
+// Instruction descriptor of an M = RM, N = n MMA, kind::f16: f32 accumulator
+// (bits 4-5 = 1), A and B bf16 (bits 7-9, 10-12 = 1), both K-major, N >> 3
+// at bit 17, M >> 4 at bit 24.
+__host__ __device__ constexpr uint32_t row_idesc(int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(RM >> 4) << 24);
+}
 
 template <int CIN, int COUT>
-struct ConvCfg {
-    static constexpr int C8 = CIN / 8;
-    static constexpr int CS = WY * HX * 16;  // bytes per chunk plane of a half window
-    static constexpr int RP = HX * 16;       // bytes per half-window row
-    static constexpr int HALF_BYTES = C8 * CS;
-    static constexpr int WIN_BYTES = 2 * HALF_BYTES;
-    static constexpr int W_BYTES = 9 * C8 * COUT * 16;
-    static constexpr uint32_t TMEM_COLS = 4 * COUT;  // one tile's accumulators
-    // Instruction descriptor, kind::f16: f32 accumulator (bits 4-5 = 1), A
-    // and B bf16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17,
-    // M >> 4 at bit 24.
-    static constexpr uint32_t IDESC =
-        (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(COUT >> 3) << 17) | (uint32_t(128 >> 4) << 24);
-    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && COUT <= 256, "tcgen05 shape");
+struct RowCfg {
+    static constexpr int C8 = CIN / 8, H2 = CIN / 16;
+    static constexpr int PLANE = RW * 16;              // bytes per chunk plane of an input row
+    static constexpr int ROW = C8 * PLANE;             // bytes per input row
+    static constexpr int STAGE = (2 * ROW + 127) & ~127;
+    static constexpr int NB = 3 * COUT;                // N of a full MMA: the three kernel rows stacked
+    static constexpr int W_BYTES = 3 * H2 * 2 * NB * 16;  // = 9 x CIN x COUT bf16
+    static constexpr uint32_t TMEM_COLS = kRowSlots * COUT;
+    static_assert(CIN % 16 == 0 && COUT % 16 == 0 && NB <= 256, "tcgen05 shape");
+    static_assert(TMEM_COLS >= 32 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor memory allocation");
 };
 
 // The develop output written by the head's epilogue (inference): picture
@@ -129,7 +134,7 @@ enum : int { kHidden = 0, kHeadF32 = 1, kHeadRgb = 2 };
 
 struct ConvArgs {
     const uint4* x;     // bf16 chunks [image][CIN/8][H][W]
-    const uint4* w;     // the layer's packed weights [tap][CIN/8][COUT] x 8 bf16
+    const uint4* w;     // the layer's packed weights (k_sg_pack_weights)
     const float* bias;  // [COUT]
     uint4* y;           // hidden layers: bf16 chunks [image][COUT/8][H][W]
     float* yf;          // head: f32 [image][16][H][W]
@@ -152,17 +157,24 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t 
            (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
 }
 
+// The MMA and its commit are executed by a whole converged warp, which
+// computes the (warp-uniform) addresses and descriptors; one lane, elected
+// in each instruction, issues it.
 __device__ __forceinline__ void umma_f16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     asm volatile(
-        "{\n\t.reg .pred p;\n\t"
+        "{\n\t.reg .pred p, e;\n\t"
+        "elect.sync _|e, 0xffffffff;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "@e tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
         "l"(a), "l"(b), "r"(idesc), "r"(acc));
 }
 
 __device__ __forceinline__ void umma_commit(uint32_t mbar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
-                 : "memory");
+    asm volatile(
+        "{\n\t.reg .pred e;\n\t"
+        "elect.sync _|e, 0xffffffff;\n\t"
+        "@e tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n\t}\n" ::"r"(mbar)
+        : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
@@ -194,13 +206,6 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint64
         if (global_ns() - t0 > limit_ns) return false;
     }
     return false;
-}
-
-// 16-byte global -> shared copy without a register round trip; `full`
-// false writes 16 zero bytes (nothing is read).
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool full) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(full ? 16 : 0)
-                 : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -246,39 +251,56 @@ __device__ __forceinline__ bool in_valid(const int4* valid, int b, int x, int y)
 
 // --- the convolution on the tensor cores --------------------------------------
 //
-// Warp-specialized and persistent. Each CTA walks tiles t = blockIdx.x,
-// + gridDim.x, ... with:
-//  - a producer warp: the layer's weights once (bulk copy), then each tile's
-//    input window by two TMA tensor loads (two halves of 18 x 18 pixels x
-//    CIN/8 chunks of the activation tensor, zero-filled outside the image)
-//    into a two-stage ring;
-//  - an MMA warp: per tile, 4 blocks x 9 taps x CIN/16 tcgen05.mma into one
-//    of two tensor-memory accumulators, then commits that free the window
-//    stage and publish the accumulator;
-//  - eight epilogue warps: tcgen05.ld of the accumulator (a warp reads the 32
-//    lanes of its quarter, for two of the four blocks), bias, ReLU, bf16
-//    stores; then they hand the accumulator back.
-// Stages and accumulators are passed by mbarriers (full/empty rings). Every
+// Row-streaming and warp-specialized. A work unit is a strip of RM = 128
+// output pixels (columns sx0 .. sx0 + 127) over a run of rows; a persistent
+// CTA takes units u = blockIdx.x, + gridDim.x, ... and walks each unit's
+// input rows top to bottom, two at a time (a step):
+//  - a producer warp: the layer's weights once (bulk copy), then a step's two
+//    input rows (RW = 130 pixels each: one to the left and right of the
+//    strip, every chunk) by one bulk copy per row and chunk plane into a ring
+//    of stages, zeros written in place of the pixels outside the picture;
+//  - an MMA warp (converged: it computes the descriptors as warp-uniform
+//    values, an elected lane issues): per input row y, for each column offset
+//    kx and 16-channel half, one tcgen05.mma with M = 128 (the strip's
+//    pixels; A is the row shifted by kx), K = 16 and N = 3 x COUT: B stacks
+//    the weights of kernel rows ky = 2, 1, 0, and the accumulator columns of
+//    output rows y - 1, y, y + 1 are three consecutive slots of a ring in
+//    tensor memory (two MMAs where the three slots wrap around the ring), so
+//    each window byte read serves three output rows. Output rows pair up
+//    (the slots of a pair are adjacent); a pair is complete after the step
+//    that follows the one that opened it, and a commit hands it to the
+//    epilogue;
+//  - sixteen epilogue warps in four groups of four, a group per pair slot:
+//    a warp reads its 32 lanes (pixels) of both rows with tcgen05.ld, writes
+//    zeros back with tcgen05.st (the MMAs accumulate onto them), hands the
+//    pair back, and adds the bias, applies ReLU and stores bf16 chunks (or the
+//    f32 head, or the develop output).
+// One wait and one commit per two rows keep the MMA warp issuing: an SM
+// takes one tcgen05.mma about every 60 cycles, so these M = 128, N = 96
+// products (48 cycles of tensor work each) leave it little time for anything
+// else. Stages and pairs are passed by mbarriers (full/empty rings). Every
 // wait is bounded; a wait that runs out sets the error flag and makes every
 // role stop at its next step.
 
-constexpr int kEpiWarps = 8, kProducerWarp = 8, kMmaWarp = 9;
-constexpr int kWsThreads = 32 * (kEpiWarps + 2);
-constexpr int kStages = 2, kAccs = 2;
-
-struct TileCoord {
-    int img, tx0, ty0;
+struct RowUnit {
+    int img, sx0, sy0, rows;
 };
 
-__device__ __forceinline__ TileCoord tile_coord(int t, int tiles_x, int tiles_y) {
-    const int per = tiles_x * tiles_y;
-    TileCoord c;
-    c.img = t / per;
-    const int r = t - c.img * per;
-    c.ty0 = (r / tiles_x) * TY;
-    c.tx0 = (r % tiles_x) * TX;
-    return c;
+__device__ __forceinline__ RowUnit row_unit(int u, int strips, int segs, int seg_rows, int H) {
+    const int per = strips * segs;
+    RowUnit r;
+    r.img = u / per;
+    const int k = u - r.img * per;
+    r.sy0 = (k / strips) * seg_rows;
+    r.sx0 = (k % strips) * RM;
+    r.rows = min(seg_rows, H - r.sy0);
+    return r;
 }
+
+// A unit's steps (input rows 0 .. rows + 1, two a step) and the output rows
+// it takes in the ring (rounded up to pairs).
+__device__ __forceinline__ int unit_steps(int rows) { return (rows + 3) / 2; }
+__device__ __forceinline__ int unit_ring_rows(int rows) { return (rows + 1) & ~1; }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
@@ -290,18 +312,6 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(bar) : "memory");
 }
 
-// One TMA tensor load of a half window: coordinates (element along the
-// row = 8 x pixel, y, plane); the element coordinate is a multiple of 8
-// bf16 (16 bytes), negative at the left edge (zero fill).
-__device__ __forceinline__ void tma_window(const CUtensorMap* map, uint32_t dst, uint32_t bar, int xe, int y,
-                                           int plane) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
-        "[%2];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(xe), "r"(y), "r"(plane)
-        : "memory");
-}
-
 // Contiguous global -> shared bulk copy (16-byte aligned, size a multiple of 16).
 __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
@@ -309,30 +319,51 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_
                  : "memory");
 }
 
-// One thread: the MMAs of a tile's four M blocks. The descriptors differ
-// from the window's and the weights' base descriptors only in the start
-// address (bits 0-13, 16-byte units, no carry: shared addresses stay below
-// 256 KB), so each is the base plus a constant.
+__device__ __forceinline__ void st_shared_zero16(uint32_t addr) {
+    asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(addr), "r"(0u) : "memory");
+}
+
+// Zeros into 32 lanes x N f32 columns of tensor memory.
+template <int N>
+__device__ __forceinline__ void tmem_zero(uint32_t taddr);
+template <>
+__device__ __forceinline__ void tmem_zero<32>(uint32_t taddr) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+        "%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1};" ::"r"(taddr),
+        "r"(0u)
+        : "memory");
+}
+template <>
+__device__ __forceinline__ void tmem_zero<16>(uint32_t taddr) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, %1, "
+        "%1};" ::"r"(taddr),
+        "r"(0u)
+        : "memory");
+}
+
+// One thread's view, issued by the whole MMA warp: the MMAs of input row
+// `row` (a stage's row) into blocks jlo .. jhi of the stacked N (block j:
+// output row y - 1 + j, kernel row ky = 2 - j), block jlo's slot s0 (a block
+// past the ring's end continues at slot 0). The descriptors differ from the
+// row's and the weights' base descriptors only in the start address (bits
+// 0-13, 16-byte units, no carry: shared addresses stay below 256 KB).
 template <int CIN, int COUT>
-__device__ __forceinline__ void issue_tile(uint32_t win_a, uint32_t w_a, uint32_t tmem) {
-    using C = ConvCfg<CIN, COUT>;
-    const uint64_t a0 = sdesc(win_a, C::CS, C::RP), b0 = sdesc(w_a, COUT * 16, 128);
+__device__ __forceinline__ void issue_row(uint32_t row, uint32_t w, uint32_t tmem, int s0, int jlo, int jhi) {
+    using C = RowCfg<CIN, COUT>;
+    const int nblk = jhi - jlo + 1, n1 = min(nblk, kRowSlots - s0);
+    // A: row m = pixel sx0 - 1 + m + kx, 8-pixel groups 128 bytes apart, the
+    // second K chunk the next chunk plane. B: [kx][half][K chunk][N][8].
+    const uint64_t a0 = sdesc(row, C::PLANE, 128), b0 = sdesc(w, C::NB * 16, 128) + (uint32_t(jlo * COUT * 16) >> 4);
 #pragma unroll
-    for (int bk = 0; bk < 4; bk++) {
+    for (int kx = 0; kx < 3; kx++) {
 #pragma unroll
-        for (int t = 0; t < 9; t++) {
-#pragma unroll
-            for (int h = 0; h < C::C8 / 2; h++) {
-                // A: rows m = 8 * r + i are window pixel (r + dy, 8 bk + i + dx),
-                // i.e. column 8 (bk & 1) + i + dx of half bk >> 1; K chunk k =
-                // the half's chunk plane 2 h + k.
-                const uint32_t aoff = uint32_t((bk >> 1) * C::HALF_BYTES + (2 * h) * C::CS + (t / 3) * C::RP +
-                                               (8 * (bk & 1) + t % 3) * 16) >> 4;
-                // B: rows n = output channel, K chunk k = weights of input
-                // channels 16 h + 8 k .. + 7 at this tap.
-                const uint32_t boff = uint32_t((t * C::C8 + 2 * h) * COUT * 16) >> 4;
-                umma_f16(tmem + uint32_t(bk * COUT), a0 + aoff, b0 + boff, C::IDESC, (t | h) != 0 ? 1u : 0u);
-            }
+        for (int h = 0; h < C::H2; h++) {
+            const uint64_t ad = a0 + (uint32_t(2 * h * C::PLANE + kx * 16) >> 4);
+            const uint64_t bd = b0 + (uint32_t((kx * C::H2 + h) * 2 * C::NB * 16) >> 4);
+            umma_f16(tmem + uint32_t(s0 * COUT), ad, bd, row_idesc(n1 * COUT), 1u);
+            if (n1 < nblk) umma_f16(tmem, ad, bd + (uint32_t(n1 * COUT * 16) >> 4), row_idesc((nblk - n1) * COUT), 1u);
         }
     }
 }
@@ -375,170 +406,251 @@ __device__ __forceinline__ void rgb_quad(const RgbOut& o, int i, int j, int wq, 
         }
 }
 
-template <int CIN, int COUT, int MODE>
-__device__ __forceinline__ void epilogue(const ConvArgs& a, const RgbOut& o, TileCoord tc, uint32_t tmem,
-                                         const float* bias) {
-    // A warp reads the 32 accumulator lanes of its quarter (the lanes tensor
-    // memory lets it access), for two of the four blocks.
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, quarter = warp & 3;
-    const int m = 32 * quarter + lane;  // accumulator row of this thread
-    const int py = tc.ty0 + (m >> 3);
-#pragma unroll 1
-    for (int bk = 2 * (warp >> 2); bk < 2 * (warp >> 2) + 2; bk++) {
-        const int px = tc.tx0 + 8 * bk + (m & 7);
-        uint32_t v[COUT];
-        tmem_load<COUT>(tmem + (uint32_t(32 * quarter) << 16) + uint32_t(bk * COUT), v);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (py >= a.H || px >= a.W) continue;
-        const bool keep = in_valid(a.valid, tc.img, px, py);
-        if (MODE == kHeadRgb) {
-            float hv[COUT];
+// One output pixel from its accumulator values v: bias, then ReLU and bf16
+// chunks (hidden), the f32 head, or the develop output.
+template <int COUT, int MODE>
+__device__ __forceinline__ void store_pixel(const ConvArgs& a, const RgbOut& o, int img, int px, int py,
+                                            const uint32_t* v, const float* bias) {
+    const bool keep = in_valid(a.valid, img, px, py);
+    if (MODE == kHeadRgb) {
+        float hv[COUT];
 #pragma unroll
-            for (int c = 0; c < COUT; c++) hv[c] = __fadd_rn(__uint_as_float(v[c]), bias[c]);
-            rgb_quad(o, px, py, a.W, a.H, hv);
-        } else if (MODE == kHeadF32) {
-            float* of = a.yf + (size_t(tc.img) * kHead * a.H + py) * a.W + px;
+        for (int c = 0; c < COUT; c++) hv[c] = __fadd_rn(__uint_as_float(v[c]), bias[c]);
+        rgb_quad(o, px, py, a.W, a.H, hv);
+    } else if (MODE == kHeadF32) {
+        float* of = a.yf + (size_t(img) * kHead * a.H + py) * a.W + px;
 #pragma unroll
-            for (int c = 0; c < COUT; c++)
-                of[size_t(c) * a.H * a.W] = keep ? __fadd_rn(__uint_as_float(v[c]), bias[c]) : 0.0f;
-        } else {
-            uint4* oy = a.y + (size_t(tc.img) * (COUT / 8) * a.H + py) * a.W + px;
+        for (int c = 0; c < COUT; c++)
+            of[size_t(c) * a.H * a.W] = keep ? __fadd_rn(__uint_as_float(v[c]), bias[c]) : 0.0f;
+    } else {
+        uint4* oy = a.y + (size_t(img) * (COUT / 8) * a.H + py) * a.W + px;
 #pragma unroll
-            for (int c8 = 0; c8 < COUT / 8; c8++) {
-                float f[8];
+        for (int c8 = 0; c8 < COUT / 8; c8++) {
+            float f[8];
 #pragma unroll
-                for (int e = 0; e < 8; e++) {
-                    const float s = __fadd_rn(__uint_as_float(v[c8 * 8 + e]), bias[c8 * 8 + e]);
-                    f[e] = keep ? fmaxf(s, 0.0f) : 0.0f;
-                }
-                oy[size_t(c8) * a.H * a.W] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
-                                                        pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
+            for (int e = 0; e < 8; e++) {
+                const float s = __fadd_rn(__uint_as_float(v[c8 * 8 + e]), bias[c8 * 8 + e]);
+                f[e] = keep ? fmaxf(s, 0.0f) : 0.0f;
             }
+            oy[size_t(c8) * a.H * a.W] = make_uint4(pack_bf16x2(f[0], f[1]), pack_bf16x2(f[2], f[3]),
+                                                    pack_bf16x2(f[4], f[5]), pack_bf16x2(f[6], f[7]));
         }
     }
 }
 
 template <int CIN, int COUT, int MODE>
-__global__ void __launch_bounds__(kWsThreads) k_sg_conv(const __grid_constant__ CUtensorMap tmap, ConvArgs a,
-                                                         RgbOut o, int tiles_x, int tiles_y, int ntiles) {
-    using C = ConvCfg<CIN, COUT>;
+__global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o, int strips, int segs, int seg_rows,
+                                                             int nunits) {
+    using C = RowCfg<CIN, COUT>;
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bars[2 * kStages + 2 * kAccs + 1];
+    __shared__ __align__(8) uint64_t bars[2 * kRowStages + 2 * kRowPairs + 2];
     __shared__ uint32_t tmem_slot;
     __shared__ float bias_s[COUT];
     volatile __shared__ int aborted;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int first = blockIdx.x, stride = gridDim.x;
-    const int n = first < ntiles ? (ntiles - 1 - first) / stride + 1 : 0;  // this CTA's tiles
-    // Weights, then the window stages, 128-byte aligned.
+    const int n = first < nunits ? (nunits - 1 - first) / stride + 1 : 0;  // this CTA's units
+    // Weights, then the stages, 128-byte aligned.
     const uint32_t wsm = smem_u32(smem);
-    const uint32_t win0 = wsm + uint32_t((C::W_BYTES + 127) & ~127);
-    const uint32_t win_stride = uint32_t((C::WIN_BYTES + 127) & ~127);
+    const uint32_t st0 = wsm + uint32_t((C::W_BYTES + 127) & ~127);
     auto bar = [&](int i) { return smem_u32(&bars[i]); };
-    // bars: full[s] = 0..1, empty[s] = 2..3, tfull[a] = 4..5, tempty[a] = 6..7, weights = 8.
-    const uint32_t full0 = bar(0), empty0 = bar(kStages), tfull0 = bar(2 * kStages), tempty0 = bar(2 * kStages + kAccs),
-                   wbar = bar(2 * kStages + 2 * kAccs);
+    // bars: stage full / empty, pair full / empty, weights, drain.
+    const uint32_t sfull0 = bar(0), sempty0 = bar(kRowStages), ofull0 = bar(2 * kRowStages),
+                   oempty0 = bar(2 * kRowStages + kRowPairs), wbar = bar(2 * kRowStages + 2 * kRowPairs),
+                   dbar = bar(2 * kRowStages + 2 * kRowPairs + 1);
     if (tid == 0) {
-        for (int s = 0; s < kStages; s++) {
-            mbar_init(full0 + 8 * s, 1);   // the producer's expect_tx arrival
-            mbar_init(empty0 + 8 * s, 1);  // the MMA warp's commit
+        for (int s = 0; s < kRowStages; s++) {
+            mbar_init(sfull0 + 8 * s, 1);   // the producer's (expect_tx) arrival
+            mbar_init(sempty0 + 8 * s, 1);  // the MMA warp's commit
         }
-        for (int q = 0; q < kAccs; q++) {
-            mbar_init(tfull0 + 8 * q, 1);           // the MMA warp's commit
-            mbar_init(tempty0 + 8 * q, kEpiWarps);  // one arrival per epilogue warp
+        for (int q = 0; q < kRowPairs; q++) {
+            mbar_init(ofull0 + 8 * q, 1);   // the MMA warp's commit
+            mbar_init(oempty0 + 8 * q, 4);  // the four warps of the pair's epilogue group
         }
         mbar_init(wbar, 1);
+        mbar_init(dbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         aborted = 0;
     }
     if (tid < COUT) bias_s[tid] = a.bias[tid];
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                     "r"(kAccs * C::TMEM_COLS));
+                     "r"(C::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    int issued = 0;  // MMA warp: tiles whose MMAs are issued
+    int filled = 0;  // producer: stages filled
 
-    if (warp == kProducerWarp) {
+    if (warp == kRowProducerWarp) {
+        bool ok = true;
         if (lane == 0) {
             mbar_expect_tx(wbar, uint32_t(C::W_BYTES));
             bulk_copy(wsm, a.w, uint32_t(C::W_BYTES), wbar);
-            for (int i = 0; i < n; i++) {
-                const int s = i % kStages;
-                // The stage is free once the MMAs of tile i - kStages are done
-                // (the first round passes: its parity refers to the phase
-                // before the barrier's first).
-                if (aborted || !mbar_wait(empty0 + 8 * s, uint32_t(((i / kStages) & 1) ^ 1), kWaitNs)) {
-                    if (!aborted) atomicOr(a.error, 1u);
-                    aborted = 1;
+        }
+        for (int u = 0; ok && u < n; u++) {
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, a.H);
+            // Pixels xa .. xb - 1 are in the picture; window column c is pixel sx0 - 1 + c.
+            const int xa = max(ru.sx0 - 1, 0), xb = min(ru.sx0 - 1 + RW, a.W);
+            const int zl = xa - (ru.sx0 - 1), zr = ru.sx0 - 1 + RW - xb, nz = zl + zr;
+            const uint32_t row_bytes = uint32_t(xb - xa) * 16;
+            for (int t = 0; t < unit_steps(ru.rows); t++) {
+                const int s = filled % kRowStages;
+                // The stage is free once the MMAs of step filled - kRowStages
+                // are done (the first round passes: its parity refers to the
+                // phase before the barrier's first).
+                int got = 1;
+                if (lane == 0)
+                    got = !aborted && mbar_wait(sempty0 + 8 * s, uint32_t(((filled / kRowStages) & 1) ^ 1), kWaitNs);
+                if (!__shfl_sync(0xFFFFFFFFu, got, 0)) {
+                    ok = false;
                     break;
                 }
-                const TileCoord tc = tile_coord(first + i * stride, tiles_x, tiles_y);
-                mbar_expect_tx(full0 + 8 * s, uint32_t(C::WIN_BYTES));
-                const uint32_t dst = win0 + uint32_t(s) * win_stride;
-                tma_window(&tmap, dst, full0 + 8 * s, 8 * (tc.tx0 - 1), tc.ty0 - 1, tc.img * C::C8);
-                tma_window(&tmap, dst + uint32_t(C::HALF_BYTES), full0 + 8 * s, 8 * (tc.tx0 + 15), tc.ty0 - 1,
-                           tc.img * C::C8);
+                const uint32_t dst = st0 + uint32_t(s * C::STAGE);
+                bool in[2];
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int i = 2 * t + e, y = ru.sy0 - 1 + i;
+                    in[e] = i <= ru.rows + 1 && y >= 0 && y < a.H;
+                }
+                if (nz > 0 && (in[0] || in[1])) {
+                    for (int e = 0; e < 2; e++) {
+                        if (!in[e]) continue;
+                        for (int z = lane; z < C::C8 * nz; z += 32) {
+                            const int p = z / nz, c = z - p * nz;
+                            st_shared_zero16(dst + uint32_t(e * C::ROW + p * C::PLANE + (c < zl ? c : RW - nz + c) * 16));
+                        }
+                    }
+                    // The zeros are read by the tensor cores (the async proxy).
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                }
+                __syncwarp();
+                if (lane == 0) {
+                    const uint32_t bytes = uint32_t(C::C8) * row_bytes * uint32_t(int(in[0]) + int(in[1]));
+                    if (bytes == 0) {
+                        mbar_arrive(sfull0 + 8 * s);
+                    } else {
+                        mbar_expect_tx(sfull0 + 8 * s, bytes);
+                        for (int e = 0; e < 2; e++) {
+                            if (!in[e]) continue;
+                            const int y = ru.sy0 - 1 + 2 * t + e;
+                            const uint4* src = a.x + (size_t(ru.img) * C::C8 * a.H + y) * a.W + xa;
+                            for (int p = 0; p < C::C8; p++)
+                                bulk_copy(dst + uint32_t(e * C::ROW + p * C::PLANE + zl * 16), src + size_t(p) * a.H * a.W,
+                                          row_bytes, sfull0 + 8 * s);
+                        }
+                    }
+                }
+                filled++;
             }
         }
-    } else if (warp == kMmaWarp) {
-        if (lane == 0) {
-            bool ok = mbar_wait(wbar, 0, kWaitNs);
-            for (int i = 0; ok && i < n; i++) {
-                const int s = i % kStages, q = i % kAccs;
-                ok = !aborted && mbar_wait(full0 + 8 * s, uint32_t((i / kStages) & 1), kWaitNs) &&
-                     mbar_wait(tempty0 + 8 * q, uint32_t(((i / kAccs) & 1) ^ 1), kWaitNs);
+        if (!ok && lane == 0) {
+            if (!aborted) atomicOr(a.error, 1u);
+            aborted = 1;
+        }
+    } else if (warp == kRowMmaWarp) {
+        // The whole warp walks the schedule (converged; the warp agrees on
+        // every wait's outcome), an elected lane issues each MMA and commit.
+        bool ok = __all_sync(0xFFFFFFFFu, mbar_wait(wbar, 0, kWaitNs));
+        int kb = 0, used = 0;  // ring rows of the earlier units; stages consumed
+        for (int u = 0; ok && u < n; u++) {
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, a.H);
+            for (int t = 0; t < unit_steps(ru.rows); t++) {
+                if (2 * t < ru.rows) {
+                    // The step opens output rows 2t, 2t + 1: their pair must be
+                    // drained and zeroed (phase u of use u).
+                    const int P = kb / 2 + t;
+                    ok = __all_sync(0xFFFFFFFFu, !aborted && mbar_wait(oempty0 + 8 * (P % kRowPairs),
+                                                                       uint32_t((P / kRowPairs) & 1), kWaitNs));
+                    if (!ok) break;
+                }
+                const int s = used % kRowStages;
+                ok = __all_sync(0xFFFFFFFFu,
+                                !aborted && mbar_wait(sfull0 + 8 * s, uint32_t((used / kRowStages) & 1), kWaitNs));
                 if (!ok) break;
                 tc_fence_after();
-                issue_tile<CIN, COUT>(win0 + uint32_t(s) * win_stride, wsm, tmem + uint32_t(q) * C::TMEM_COLS);
-                umma_commit(empty0 + 8 * s);  // the window stage, once these MMAs have read it
-                umma_commit(tfull0 + 8 * q);  // the accumulator, once they are done
-                issued = i + 1;
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int i = 2 * t + e, y = ru.sy0 - 1 + i;
+                    if (i > ru.rows + 1 || y < 0 || y >= a.H) continue;
+                    // Blocks j of output rows i - 2 + j inside the unit.
+                    const int jlo = max(0, 2 - i), jhi = min(2, ru.rows + 1 - i);
+                    issue_row<CIN, COUT>(st0 + uint32_t(s * C::STAGE + e * C::ROW), wsm, tmem,
+                                         (kb + i - 2 + jlo) % kRowSlots, jlo, jhi);
+                }
+                umma_commit(sempty0 + 8 * s);  // the stage, once these MMAs have read it
+                used++;
+                // Output rows 2t - 2, 2t - 1 took their last products (from input
+                // row 2t + 1): hand the pair to the epilogue.
+                if (t >= 1) umma_commit(ofull0 + 8 * ((kb / 2 + t - 1) % kRowPairs));
             }
-            if (!ok) {
-                if (!aborted) atomicOr(a.error, 1u);
-                aborted = 1;
-            }
+            kb += unit_ring_rows(ru.rows);
+        }
+        umma_commit(dbar);  // every issued MMA
+        if (!ok && lane == 0) {
+            if (!aborted) atomicOr(a.error, 1u);
+            aborted = 1;
         }
     } else {
-        for (int i = 0; i < n; i++) {
-            const int q = i % kAccs;
-            bool ok = !aborted && mbar_wait(tfull0 + 8 * q, uint32_t((i / kAccs) & 1), kWaitNs);
-            ok = __all_sync(0xFFFFFFFFu, ok);  // the warp-collective loads need one branch per warp
-            if (!ok) {
-                if (lane == 0) {
-                    if (!aborted) atomicOr(a.error, 1u);
-                    aborted = 1;
+        const int g = warp >> 2, q = warp & 3;  // group = pair slot; lane quarter
+        const uint32_t lanes = uint32_t(32 * q) << 16;
+        const uint32_t slot0 = tmem + lanes + uint32_t(2 * g * COUT), slot1 = slot0 + uint32_t(COUT);
+        // The ring starts zeroed (phase 0 of each pair's empty barrier).
+        tmem_zero<COUT>(slot0);
+        tmem_zero<COUT>(slot1);
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(oempty0 + 8 * g);
+        int kb = 0;
+        bool ok = true;
+        for (int u = 0; ok && u < n; u++) {
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, a.H);
+            const int px = ru.sx0 + 32 * q + lane;
+            for (int p = ((g - kb / 2) % kRowPairs + kRowPairs) % kRowPairs; 2 * p < ru.rows; p += kRowPairs) {
+                const int P = kb / 2 + p;
+                bool got = !aborted && mbar_wait(ofull0 + 8 * g, uint32_t((P / kRowPairs) & 1), kWaitNs);
+                got = __all_sync(0xFFFFFFFFu, got);  // the warp-collective loads need one branch per warp
+                if (!got) {
+                    ok = false;
+                    break;
                 }
-                break;
+                tc_fence_after();
+                uint32_t v[COUT];
+                tmem_load<COUT>(slot0, v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                tmem_zero<COUT>(slot0);
+                if (px < a.W) store_pixel<COUT, MODE>(a, o, ru.img, px, ru.sy0 + 2 * p, v, bias_s);
+                tmem_load<COUT>(slot1, v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                tmem_zero<COUT>(slot1);
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(oempty0 + 8 * g);
+                if (px < a.W && 2 * p + 1 < ru.rows) store_pixel<COUT, MODE>(a, o, ru.img, px, ru.sy0 + 2 * p + 1, v, bias_s);
             }
-            tc_fence_after();
-            epilogue<CIN, COUT, MODE>(a, o, tile_coord(first + i * stride, tiles_x, tiles_y),
-                                      tmem + uint32_t(q) * C::TMEM_COLS, bias_s);
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(tempty0 + 8 * q);
+            kb += unit_ring_rows(ru.rows);
+        }
+        if (!ok && lane == 0) {
+            if (!aborted) atomicOr(a.error, 1u);
+            aborted = 1;
         }
     }
     __syncthreads();
-    if (aborted && tid == kMmaWarp * 32 && issued > 0) {
-        // Let the issued MMAs finish (bounded) before the memory is freed:
-        // they complete in order, so the last commit covers them all.
-        const int j = issued - 1;
-        mbar_wait(tfull0 + 8 * (j % kAccs), uint32_t((j / kAccs) & 1), kWaitNs);
-    }
-    if (aborted && tid == kProducerWarp * 32) {
-        // Let the issued window loads land (bounded) before the CTA exits.
-        for (int s = 0; s < kStages; s++) mbar_wait(full0 + 8 * s, 0, kWaitNs / 8);
+    if (aborted && warp == kRowMmaWarp) mbar_wait(dbar, 0, kWaitNs);  // issued MMAs finish (bounded)
+    if (aborted && tid == kRowProducerWarp * 32) {
+        // Let the issued copies land (bounded) before the CTA exits: the last
+        // fill of each stage is its latest phase.
+        for (int j = max(0, filled - kRowStages); j < filled; j++)
+            mbar_wait(sfull0 + 8 * (j % kRowStages), uint32_t((j / kRowStages) & 1), kWaitNs / 8);
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kAccs * C::TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::TMEM_COLS));
 }
 
 // cuTensorMapEncodeTiled, looked up once through the runtime (no link
@@ -559,29 +671,33 @@ EncodeTiledFn encode_tiled() {
     return fn;
 }
 
-cudaError_t encode_window_map(CUtensorMap* map, const void* x, int c8, int H, int W, int images) {
-    const EncodeTiledFn fn = encode_tiled();
-    if (!fn) return cudaErrorUnknown;
-    // The activation tensor as 3-D bf16: a row of one chunk (8 channels x W
-    // pixels, contiguous), y, and (image, chunk) planes; the half-window box
-    // is HX pixels of a row, WY rows, one image's chunks.
-    const cuuint64_t dims[3] = {8 * cuuint64_t(W), cuuint64_t(H), cuuint64_t(c8) * cuuint64_t(images)};
-    const cuuint64_t strides[2] = {cuuint64_t(W) * 16, cuuint64_t(W) * cuuint64_t(H) * 16};
-    const cuuint32_t box[3] = {8 * HX, WY, cuuint32_t(c8)};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(x), dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+// Rows per work unit: the run length whose units, spread over two CTAs an
+// SM, give the fewest input rows to the busiest CTA (a unit of S rows reads
+// S + 2; a CTA's rows follow one another through its pipeline, so a CTA, not
+// an SM, sets the pace).
+int row_segment(int strips, int H, int images, int sms) {
+    int best = H;
+    long best_cost = LONG_MAX;
+    for (int S = 8;; S += 8) {
+        const int rows = std::min(S, H), segs = (H + rows - 1) / rows;
+        const long units = long(strips) * segs * images;
+        const long cost = (units + 2L * sms - 1) / (2L * sms) * (rows + 2);
+        if (cost < best_cost) {
+            best_cost = cost;
+            best = rows;
+        }
+        if (S >= H) break;
+    }
+    return best;
 }
 
 template <int CIN, int COUT, int MODE>
 cudaError_t conv_launch(const ConvArgs& a, const RgbOut& o, int images, cudaStream_t s) {
-    using C = ConvCfg<CIN, COUT>;
-    // Weights and two window stages; at least 80 KB, so that no more than
-    // two CTAs share an SM: two CTAs' 2 x 4 x COUT accumulator columns fit
-    // in its 512, and a third CTA's allocation would wait for one of them.
-    constexpr int smem = std::max(((C::W_BYTES + 127) & ~127) + kStages * ((C::WIN_BYTES + 127) & ~127), 80 * 1024);
+    using C = RowCfg<CIN, COUT>;
+    // Weights and the row stages; at least 80 KB, so that no more than two
+    // CTAs share an SM (their accumulator rings fit in its 512 tensor-memory
+    // columns; a third CTA's allocation would wait for one of them).
+    constexpr int smem = std::max(((C::W_BYTES + 127) & ~127) + kRowStages * C::STAGE, 80 * 1024);
     // The shared-memory limit and the SM count, set and read once per device
     // (kept per device in atomics: contexts on several threads launch too).
     static std::atomic<int> sms_of[kMaxDevices];
@@ -591,18 +707,19 @@ cudaError_t conv_launch(const ConvArgs& a, const RgbOut& o, int images, cudaStre
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     int sms = sms_of[dev].load(std::memory_order_acquire);
     if (sms == 0) {
-        e = cudaFuncSetAttribute(k_sg_conv<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        e = cudaFuncSetAttribute(k_sg_rows<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
         sms_of[dev].store(sms, std::memory_order_release);
     }
-    alignas(64) CUtensorMap map;
-    const cudaError_t em = encode_window_map(&map, a.x, C::C8, a.H, a.W, images);
-    if (em != cudaSuccess) return em;
-    const int tiles_x = (a.W + TX - 1) / TX, tiles_y = (a.H + TY - 1) / TY;
-    const int ntiles = tiles_x * tiles_y * images;
-    const int grid = std::max(1, std::min(ntiles, 2 * sms));
-    k_sg_conv<CIN, COUT, MODE><<<grid, kWsThreads, smem, s>>>(map, a, o, tiles_x, tiles_y, ntiles);
+    if (a.W <= 0 || a.H <= 0 || images <= 0) return cudaErrorInvalidValue;
+    const int strips = (a.W + RM - 1) / RM;
+    const int seg_rows = row_segment(strips, a.H, images, sms);
+    const int segs = (a.H + seg_rows - 1) / seg_rows;
+    const long nunits = long(strips) * segs * images;
+    if (nunits > INT_MAX) return cudaErrorInvalidValue;
+    const int grid = int(std::max(1L, std::min(nunits, 2L * sms)));
+    k_sg_rows<CIN, COUT, MODE><<<grid, kRowThreads, smem, s>>>(a, o, strips, segs, seg_rows, int(nunits));
     count_launch();
     return cudaGetLastError();
 }
@@ -679,18 +796,26 @@ __global__ void k_sg_pack(PackArgs p) {
     }
 }
 
-// f32 parameters -> bf16 weights in the tensor cores' B layout, all layers.
+// f32 parameters -> bf16 weights in the tensor cores' B layout, all layers:
+// per column offset kx and 16-channel half, two K chunks of N = 3 x cout
+// rows (block j of cout rows: kernel row ky = 2 - j) of 8 input channels.
 __global__ void k_sg_pack_weights(const float* __restrict__ params, uint16_t* __restrict__ packed) {
     const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= kPacked) return;
     int l = 0;
     while (l < kLayers - 1 && i >= packed_off(l + 1)) l++;
-    const int cin = cin_of(l), cout = cout_of(l);
-    const size_t k = i - packed_off(l);
-    // k = ((tap * cin/8 + kc) * cout + n) * 8 + e
-    const int e = int(k % 8), n = int((k / 8) % cout);
-    const int kc = int((k / 8 / cout) % (cin / 8)), tap = int(k / 8 / cout / (cin / 8));
-    const float wv = params[layer_off(l) + (size_t(n) * cin + kc * 8 + e) * 9 + tap];
+    const int cin = cin_of(l), cout = cout_of(l), nb = 3 * cout;
+    // k = (((kx * cin/16 + h) * 2 + kc) * nb + n) * 8 + e
+    size_t k = i - packed_off(l);
+    const int e = int(k % 8);
+    k /= 8;
+    const int n = int(k % nb);
+    k /= nb;
+    const int kc = int(k % 2);
+    k /= 2;
+    const int h = int(k % (cin / 16)), kx = int(k / (cin / 16));
+    const int co = n % cout, ky = 2 - n / cout, ci = 16 * h + 8 * kc + e;
+    const float wv = params[layer_off(l) + (size_t(co) * cin + ci) * 9 + ky * 3 + kx];
     packed[i] = __bfloat16_as_ushort(__float2bfloat16_rn(wv));
 }
 

@@ -42,7 +42,9 @@ def random_image(rng, hq, wq):
     return in16, base, target
 
 
-@pytest.mark.parametrize("hq,wq", [(40, 70), (16, 32), (7, 9)])
+# Shapes: one strip of 128 pixels and one run of rows; three strips (the
+# last 4 pixels wide) over runs of a few rows; a last strip of one pixel.
+@pytest.mark.parametrize("hq,wq", [(40, 70), (16, 32), (7, 9), (70, 260), (33, 129), (1, 5)])
 def test_forward_matches_the_oracle(hq, wq):
     rng = np.random.default_rng(hq * wq)
     in16, base, target = random_image(rng, hq, wq)
