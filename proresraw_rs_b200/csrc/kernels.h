@@ -147,7 +147,7 @@ struct DevelopDesc {
     float* b;
     // Non-null: develop only the 32x32 tiles whose byte is nonzero (row-major
     // over the tile grid).
-    const uint8_t* tile_mask;
+    const unsigned* tile_mask;
     // Nonzero: at most this many CTAs per SM (shared memory reserved per
     // CTA), leaving room for kernels of other streams.
     uint32_t ctas_per_sm;

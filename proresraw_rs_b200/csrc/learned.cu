@@ -86,9 +86,14 @@ constexpr uint64_t kWaitNs = 1000000000ull;  // 1 s
 // Row-streaming convolution (k_sg_rows below): a CTA computes strips of RM
 // output pixels of a run of rows; an input row of a strip is RW pixels.
 constexpr int RM = 128, RW = RM + 2;
-constexpr int kRowSlots = 8;                 // accumulator ring in tensor memory, output rows
-constexpr int kRowPairs = kRowSlots / 2;     // ... as pairs of adjacent rows
-constexpr int kRowStages = 4;                // ring of shared-memory stages, two input rows each
+// Ring sizes of a layer's pipeline: accumulator rows in tensor memory (as
+// pairs of adjacent rows) and shared-memory stages of two input rows.
+template <int SLOTS, int STAGES>
+struct Ring {
+    static constexpr int slots = SLOTS, pairs = SLOTS / 2, stages = STAGES;
+};
+using Ring1 = Ring<8, 4>;  // one layer a CTA, two CTAs an SM
+constexpr int kRowSlots = Ring1::slots, kRowPairs = Ring1::pairs, kRowStages = Ring1::stages;
 constexpr int kRowEpiWarps = 4 * kRowPairs;  // an epilogue group of four warps (128 lanes) per pair
 constexpr int kRowProducerWarp = kRowEpiWarps, kRowMmaWarp = kRowEpiWarps + 1;
 constexpr int kRowThreads = 32 * (kRowEpiWarps + 2);
@@ -100,15 +105,22 @@ __host__ __device__ constexpr uint32_t row_idesc(int n) {
     return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(RM >> 4) << 24);
 }
 
-template <int CIN, int COUT>
-struct RowCfg {
+// Input rows of CIN channels in shared memory: per row, CIN / 8 chunk
+// planes of RW 16-byte pixels; two rows a stage.
+template <int CIN>
+struct RowIn {
     static constexpr int C8 = CIN / 8, H2 = CIN / 16;
-    static constexpr int PLANE = RW * 16;              // bytes per chunk plane of an input row
-    static constexpr int ROW = C8 * PLANE;             // bytes per input row
+    static constexpr int PLANE = RW * 16;   // bytes per chunk plane of an input row
+    static constexpr int ROW = C8 * PLANE;  // bytes per input row
     static constexpr int STAGE = (2 * ROW + 127) & ~127;
+};
+
+template <int CIN, int COUT>
+struct RowCfg : RowIn<CIN> {
+    using RowIn<CIN>::H2;
     static constexpr int NB = 3 * COUT;                // N of a full MMA: the three kernel rows stacked
     static constexpr int W_BYTES = 3 * H2 * 2 * NB * 16;  // = 9 x CIN x COUT bf16
-    static constexpr uint32_t TMEM_COLS = kRowSlots * COUT;
+    static constexpr uint32_t TMEM_COLS = kRowSlots * COUT;  // one layer a CTA (Ring1)
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && NB <= 256, "tcgen05 shape");
     static_assert(TMEM_COLS >= 32 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor memory allocation");
 };
@@ -125,7 +137,7 @@ struct RgbOut {
     float* r;
     float* g;
     float* b;
-    const uint8_t* fallback;  // per 32x32 picture tile: developed by the plain kernel instead
+    const unsigned* fallback;  // per 32x32 picture tile: developed by the plain kernel instead
     int tiles_x;
 };
 
@@ -286,13 +298,13 @@ struct RowUnit {
     int img, sx0, sy0, rows;
 };
 
-__device__ __forceinline__ RowUnit row_unit(int u, int strips, int segs, int seg_rows, int H) {
+__device__ __forceinline__ RowUnit row_unit(int u, int strips, int segs, int seg_rows, int strip_w, int H) {
     const int per = strips * segs;
     RowUnit r;
     r.img = u / per;
     const int k = u - r.img * per;
     r.sy0 = (k / strips) * seg_rows;
-    r.sx0 = (k % strips) * RM;
+    r.sx0 = (k % strips) * strip_w;
     r.rows = min(seg_rows, H - r.sy0);
     return r;
 }
@@ -349,10 +361,10 @@ __device__ __forceinline__ void tmem_zero<16>(uint32_t taddr) {
 // past the ring's end continues at slot 0). The descriptors differ from the
 // row's and the weights' base descriptors only in the start address (bits
 // 0-13, 16-byte units, no carry: shared addresses stay below 256 KB).
-template <int CIN, int COUT>
+template <int CIN, int COUT, class R>
 __device__ __forceinline__ void issue_row(uint32_t row, uint32_t w, uint32_t tmem, int s0, int jlo, int jhi) {
     using C = RowCfg<CIN, COUT>;
-    const int nblk = jhi - jlo + 1, n1 = min(nblk, kRowSlots - s0);
+    const int nblk = jhi - jlo + 1, n1 = min(nblk, R::slots - s0);
     // A: row m = pixel sx0 - 1 + m + kx, 8-pixel groups 128 bytes apart, the
     // second K chunk the next chunk plane. B: [kx][half][K chunk][N][8].
     const uint64_t a0 = sdesc(row, C::PLANE, 128), b0 = sdesc(w, C::NB * 16, 128) + (uint32_t(jlo * COUT * 16) >> 4);
@@ -438,6 +450,166 @@ __device__ __forceinline__ void store_pixel(const ConvArgs& a, const RgbOut& o, 
     }
 }
 
+// The input rows of a unit as one pipeline reads them: rows y0 .. y0 + nin - 1
+// (those inside the picture), window column c = pixel xw + c, two rows a
+// stage.
+struct RowSpan {
+    int img, xw, y0, nin;
+};
+
+// Producer warp: the span's rows into the stage ring, one bulk copy per row
+// and chunk plane, zeros in place of the pixels outside the picture. False
+// when a wait ran out.
+template <int CIN, class R>
+__device__ __forceinline__ bool produce_span(const ConvArgs& a, const RowSpan& sp, uint32_t st0, uint32_t sfull0,
+                                             uint32_t sempty0, int& filled, volatile int& aborted, int lane) {
+    using I = RowIn<CIN>;
+    const int xa = max(sp.xw, 0), xb = min(sp.xw + RW, a.W);
+    const int zl = xa - sp.xw, zr = sp.xw + RW - xb, nz = zl + zr;
+    const uint32_t row_bytes = uint32_t(xb - xa) * 16;
+    for (int t = 0; 2 * t < sp.nin; t++) {
+        const int s = filled % R::stages;
+        // The stage is free once the MMAs of fill filled - R::stages are done
+        // (the first round passes: its parity refers to the phase before the
+        // barrier's first).
+        int got = 1;
+        if (lane == 0) got = !aborted && mbar_wait(sempty0 + 8 * s, uint32_t(((filled / R::stages) & 1) ^ 1), kWaitNs);
+        if (!__shfl_sync(0xFFFFFFFFu, got, 0)) return false;
+        const uint32_t dst = st0 + uint32_t(s * I::STAGE);
+        bool in[2];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int i = 2 * t + e, y = sp.y0 + i;
+            in[e] = i < sp.nin && y >= 0 && y < a.H;
+        }
+        if (nz > 0 && (in[0] || in[1])) {
+            for (int e = 0; e < 2; e++) {
+                if (!in[e]) continue;
+                for (int z = lane; z < I::C8 * nz; z += 32) {
+                    const int p = z / nz, c = z - p * nz;
+                    st_shared_zero16(dst + uint32_t(e * I::ROW + p * I::PLANE + (c < zl ? c : RW - nz + c) * 16));
+                }
+            }
+            // The zeros are read by the tensor cores (the async proxy).
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const uint32_t bytes = uint32_t(I::C8) * row_bytes * uint32_t(int(in[0]) + int(in[1]));
+            if (bytes == 0) {
+                mbar_arrive(sfull0 + 8 * s);
+            } else {
+                mbar_expect_tx(sfull0 + 8 * s, bytes);
+                for (int e = 0; e < 2; e++) {
+                    if (!in[e]) continue;
+                    const uint4* src = a.x + (size_t(sp.img) * I::C8 * a.H + (sp.y0 + 2 * t + e)) * a.W + xa;
+                    for (int p = 0; p < I::C8; p++)
+                        bulk_copy(dst + uint32_t(e * I::ROW + p * I::PLANE + zl * 16), src + size_t(p) * a.H * a.W,
+                                  row_bytes, sfull0 + 8 * s);
+                }
+            }
+        }
+        filled++;
+    }
+    return true;
+}
+
+// Barriers of one layer's pipeline: its input stages (full / empty) and its
+// accumulator pairs (full / empty), R::stages and R::pairs of each.
+struct RowBars {
+    uint32_t sfull, sempty, ofull, oempty;
+};
+
+// MMA warp (converged; an elected lane issues): one unit of one layer, output
+// rows 0 .. rows - 1 (ring rows kb ..), input row i = row y0 + i of the
+// picture (rows outside it give nothing), read from stage ring st0 with
+// stages stage_bytes apart. False when a wait ran out.
+template <int CIN, int COUT, class R>
+__device__ __forceinline__ bool mma_unit(int rows, int y0, int H, uint32_t st0, int stage_bytes, const RowBars& b,
+                                         uint32_t w, uint32_t tmem, int& kb, int& used, volatile int& aborted) {
+    using C = RowCfg<CIN, COUT>;
+    for (int t = 0; t < unit_steps(rows); t++) {
+        if (2 * t < rows) {
+            // The step opens output rows 2t, 2t + 1: their pair must be
+            // drained and zeroed (phase u of use u).
+            const int P = kb / 2 + t;
+            if (!__all_sync(0xFFFFFFFFu, !aborted && mbar_wait(b.oempty + 8 * (P % R::pairs),
+                                                               uint32_t((P / R::pairs) & 1), kWaitNs)))
+                return false;
+        }
+        const int s = used % R::stages;
+        if (!__all_sync(0xFFFFFFFFu, !aborted && mbar_wait(b.sfull + 8 * s, uint32_t((used / R::stages) & 1), kWaitNs)))
+            return false;
+        tc_fence_after();
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int i = 2 * t + e, y = y0 + i;
+            if (i > rows + 1 || y < 0 || y >= H) continue;
+            // Blocks j of output rows i - 2 + j inside the unit.
+            const int jlo = max(0, 2 - i), jhi = min(2, rows + 1 - i);
+            issue_row<CIN, COUT, R>(st0 + uint32_t(s * stage_bytes + e * C::ROW), w, tmem, (kb + i - 2 + jlo) % R::slots,
+                                    jlo, jhi);
+        }
+        umma_commit(b.sempty + 8 * s);  // the stage, once these MMAs have read it
+        used++;
+        // Output rows 2t - 2, 2t - 1 took their last products (from input row
+        // 2t + 1): hand the pair to the epilogue.
+        if (t >= 1) umma_commit(b.ofull + 8 * ((kb / 2 + t - 1) % R::pairs));
+    }
+    kb += unit_ring_rows(rows);
+    return true;
+}
+
+// Epilogue warp: wait for ring pair P (slot pair P % R::pairs) and read
+// its first row; the caller reads the second with pair_second.
+template <int COUT, class R>
+__device__ __forceinline__ bool pair_first(const RowBars& b, int P, uint32_t slot0, uint32_t* v, volatile int& aborted) {
+    bool got = !aborted && mbar_wait(b.ofull + 8 * (P % R::pairs), uint32_t((P / R::pairs) & 1), kWaitNs);
+    if (!__all_sync(0xFFFFFFFFu, got)) return false;  // the warp-collective loads need one branch per warp
+    tc_fence_after();
+    tmem_load<COUT>(slot0, v);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    tmem_zero<COUT>(slot0);  // the MMAs accumulate onto zeros
+    return true;
+}
+
+// The pair's second row into v; the pair goes back to the MMA warp.
+template <int COUT, class R>
+__device__ __forceinline__ void pair_second(const RowBars& b, int P, uint32_t slot1, uint32_t* v, int lane) {
+    tmem_load<COUT>(slot1, v);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    tmem_zero<COUT>(slot1);
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(b.oempty + 8 * (P % R::pairs));
+}
+
+// The ring's pair slot g of a warp's lane quarter starts zeroed (phase 0 of
+// the pair's empty barrier).
+template <int COUT>
+__device__ __forceinline__ void pair_init(const RowBars& b, int g, uint32_t slot0, int lane) {
+    tmem_zero<COUT>(slot0);
+    tmem_zero<COUT>(slot0 + uint32_t(COUT));
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(b.oempty + 8 * g);
+}
+
+template <class R>
+__device__ __forceinline__ void init_bars(const RowBars& b, uint32_t full_count) {
+    for (int s = 0; s < R::stages; s++) {
+        mbar_init(b.sfull + 8 * s, full_count);  // the stage's producer arrival(s)
+        mbar_init(b.sempty + 8 * s, 1);          // the MMA warp's commit
+    }
+    for (int q = 0; q < R::pairs; q++) {
+        mbar_init(b.ofull + 8 * q, 1);   // the MMA warp's commit
+        mbar_init(b.oempty + 8 * q, 4);  // the four warps of the pair's epilogue group
+    }
+}
+
+// One layer: a CTA per pair of SMs' halves (two an SM), the roles above.
 template <int CIN, int COUT, int MODE>
 __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o, int strips, int segs, int seg_rows,
                                                              int nunits) {
@@ -454,19 +626,10 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o
     const uint32_t wsm = smem_u32(smem);
     const uint32_t st0 = wsm + uint32_t((C::W_BYTES + 127) & ~127);
     auto bar = [&](int i) { return smem_u32(&bars[i]); };
-    // bars: stage full / empty, pair full / empty, weights, drain.
-    const uint32_t sfull0 = bar(0), sempty0 = bar(kRowStages), ofull0 = bar(2 * kRowStages),
-                   oempty0 = bar(2 * kRowStages + kRowPairs), wbar = bar(2 * kRowStages + 2 * kRowPairs),
-                   dbar = bar(2 * kRowStages + 2 * kRowPairs + 1);
+    const RowBars rb{bar(0), bar(kRowStages), bar(2 * kRowStages), bar(2 * kRowStages + kRowPairs)};
+    const uint32_t wbar = bar(2 * kRowStages + 2 * kRowPairs), dbar = wbar + 8;
     if (tid == 0) {
-        for (int s = 0; s < kRowStages; s++) {
-            mbar_init(sfull0 + 8 * s, 1);   // the producer's (expect_tx) arrival
-            mbar_init(sempty0 + 8 * s, 1);  // the MMA warp's commit
-        }
-        for (int q = 0; q < kRowPairs; q++) {
-            mbar_init(ofull0 + 8 * q, 1);   // the MMA warp's commit
-            mbar_init(oempty0 + 8 * q, 4);  // the four warps of the pair's epilogue group
-        }
+        init_bars<Ring1>(rb, 1);
         mbar_init(wbar, 1);
         mbar_init(dbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -483,161 +646,47 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
     int filled = 0;  // producer: stages filled
+    bool ok = true;
 
     if (warp == kRowProducerWarp) {
-        bool ok = true;
         if (lane == 0) {
             mbar_expect_tx(wbar, uint32_t(C::W_BYTES));
             bulk_copy(wsm, a.w, uint32_t(C::W_BYTES), wbar);
         }
         for (int u = 0; ok && u < n; u++) {
-            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, a.H);
-            // Pixels xa .. xb - 1 are in the picture; window column c is pixel sx0 - 1 + c.
-            const int xa = max(ru.sx0 - 1, 0), xb = min(ru.sx0 - 1 + RW, a.W);
-            const int zl = xa - (ru.sx0 - 1), zr = ru.sx0 - 1 + RW - xb, nz = zl + zr;
-            const uint32_t row_bytes = uint32_t(xb - xa) * 16;
-            for (int t = 0; t < unit_steps(ru.rows); t++) {
-                const int s = filled % kRowStages;
-                // The stage is free once the MMAs of step filled - kRowStages
-                // are done (the first round passes: its parity refers to the
-                // phase before the barrier's first).
-                int got = 1;
-                if (lane == 0)
-                    got = !aborted && mbar_wait(sempty0 + 8 * s, uint32_t(((filled / kRowStages) & 1) ^ 1), kWaitNs);
-                if (!__shfl_sync(0xFFFFFFFFu, got, 0)) {
-                    ok = false;
-                    break;
-                }
-                const uint32_t dst = st0 + uint32_t(s * C::STAGE);
-                bool in[2];
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const int i = 2 * t + e, y = ru.sy0 - 1 + i;
-                    in[e] = i <= ru.rows + 1 && y >= 0 && y < a.H;
-                }
-                if (nz > 0 && (in[0] || in[1])) {
-                    for (int e = 0; e < 2; e++) {
-                        if (!in[e]) continue;
-                        for (int z = lane; z < C::C8 * nz; z += 32) {
-                            const int p = z / nz, c = z - p * nz;
-                            st_shared_zero16(dst + uint32_t(e * C::ROW + p * C::PLANE + (c < zl ? c : RW - nz + c) * 16));
-                        }
-                    }
-                    // The zeros are read by the tensor cores (the async proxy).
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                }
-                __syncwarp();
-                if (lane == 0) {
-                    const uint32_t bytes = uint32_t(C::C8) * row_bytes * uint32_t(int(in[0]) + int(in[1]));
-                    if (bytes == 0) {
-                        mbar_arrive(sfull0 + 8 * s);
-                    } else {
-                        mbar_expect_tx(sfull0 + 8 * s, bytes);
-                        for (int e = 0; e < 2; e++) {
-                            if (!in[e]) continue;
-                            const int y = ru.sy0 - 1 + 2 * t + e;
-                            const uint4* src = a.x + (size_t(ru.img) * C::C8 * a.H + y) * a.W + xa;
-                            for (int p = 0; p < C::C8; p++)
-                                bulk_copy(dst + uint32_t(e * C::ROW + p * C::PLANE + zl * 16), src + size_t(p) * a.H * a.W,
-                                          row_bytes, sfull0 + 8 * s);
-                        }
-                    }
-                }
-                filled++;
-            }
-        }
-        if (!ok && lane == 0) {
-            if (!aborted) atomicOr(a.error, 1u);
-            aborted = 1;
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, RM, a.H);
+            ok = produce_span<CIN, Ring1>(a, RowSpan{ru.img, ru.sx0 - 1, ru.sy0 - 1, ru.rows + 2}, st0, rb.sfull, rb.sempty,
+                                   filled, aborted, lane);
         }
     } else if (warp == kRowMmaWarp) {
-        // The whole warp walks the schedule (converged; the warp agrees on
-        // every wait's outcome), an elected lane issues each MMA and commit.
-        bool ok = __all_sync(0xFFFFFFFFu, mbar_wait(wbar, 0, kWaitNs));
+        ok = __all_sync(0xFFFFFFFFu, mbar_wait(wbar, 0, kWaitNs));
         int kb = 0, used = 0;  // ring rows of the earlier units; stages consumed
         for (int u = 0; ok && u < n; u++) {
-            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, a.H);
-            for (int t = 0; t < unit_steps(ru.rows); t++) {
-                if (2 * t < ru.rows) {
-                    // The step opens output rows 2t, 2t + 1: their pair must be
-                    // drained and zeroed (phase u of use u).
-                    const int P = kb / 2 + t;
-                    ok = __all_sync(0xFFFFFFFFu, !aborted && mbar_wait(oempty0 + 8 * (P % kRowPairs),
-                                                                       uint32_t((P / kRowPairs) & 1), kWaitNs));
-                    if (!ok) break;
-                }
-                const int s = used % kRowStages;
-                ok = __all_sync(0xFFFFFFFFu,
-                                !aborted && mbar_wait(sfull0 + 8 * s, uint32_t((used / kRowStages) & 1), kWaitNs));
-                if (!ok) break;
-                tc_fence_after();
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const int i = 2 * t + e, y = ru.sy0 - 1 + i;
-                    if (i > ru.rows + 1 || y < 0 || y >= a.H) continue;
-                    // Blocks j of output rows i - 2 + j inside the unit.
-                    const int jlo = max(0, 2 - i), jhi = min(2, ru.rows + 1 - i);
-                    issue_row<CIN, COUT>(st0 + uint32_t(s * C::STAGE + e * C::ROW), wsm, tmem,
-                                         (kb + i - 2 + jlo) % kRowSlots, jlo, jhi);
-                }
-                umma_commit(sempty0 + 8 * s);  // the stage, once these MMAs have read it
-                used++;
-                // Output rows 2t - 2, 2t - 1 took their last products (from input
-                // row 2t + 1): hand the pair to the epilogue.
-                if (t >= 1) umma_commit(ofull0 + 8 * ((kb / 2 + t - 1) % kRowPairs));
-            }
-            kb += unit_ring_rows(ru.rows);
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, RM, a.H);
+            ok = mma_unit<CIN, COUT, Ring1>(ru.rows, ru.sy0 - 1, a.H, st0, C::STAGE, rb, wsm, tmem, kb, used, aborted);
         }
         umma_commit(dbar);  // every issued MMA
-        if (!ok && lane == 0) {
-            if (!aborted) atomicOr(a.error, 1u);
-            aborted = 1;
-        }
     } else {
         const int g = warp >> 2, q = warp & 3;  // group = pair slot; lane quarter
-        const uint32_t lanes = uint32_t(32 * q) << 16;
-        const uint32_t slot0 = tmem + lanes + uint32_t(2 * g * COUT), slot1 = slot0 + uint32_t(COUT);
-        // The ring starts zeroed (phase 0 of each pair's empty barrier).
-        tmem_zero<COUT>(slot0);
-        tmem_zero<COUT>(slot1);
-        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(oempty0 + 8 * g);
+        const uint32_t slot0 = tmem + (uint32_t(32 * q) << 16) + uint32_t(2 * g * COUT), slot1 = slot0 + uint32_t(COUT);
+        pair_init<COUT>(rb, g, slot0, lane);
         int kb = 0;
-        bool ok = true;
         for (int u = 0; ok && u < n; u++) {
-            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, a.H);
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, RM, a.H);
             const int px = ru.sx0 + 32 * q + lane;
             for (int p = ((g - kb / 2) % kRowPairs + kRowPairs) % kRowPairs; 2 * p < ru.rows; p += kRowPairs) {
-                const int P = kb / 2 + p;
-                bool got = !aborted && mbar_wait(ofull0 + 8 * g, uint32_t((P / kRowPairs) & 1), kWaitNs);
-                got = __all_sync(0xFFFFFFFFu, got);  // the warp-collective loads need one branch per warp
-                if (!got) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
                 uint32_t v[COUT];
-                tmem_load<COUT>(slot0, v);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                tmem_zero<COUT>(slot0);
+                if (!(ok = pair_first<COUT, Ring1>(rb, kb / 2 + p, slot0, v, aborted))) break;
                 if (px < a.W) store_pixel<COUT, MODE>(a, o, ru.img, px, ru.sy0 + 2 * p, v, bias_s);
-                tmem_load<COUT>(slot1, v);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                tmem_zero<COUT>(slot1);
-                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(oempty0 + 8 * g);
+                pair_second<COUT, Ring1>(rb, kb / 2 + p, slot1, v, lane);
                 if (px < a.W && 2 * p + 1 < ru.rows) store_pixel<COUT, MODE>(a, o, ru.img, px, ru.sy0 + 2 * p + 1, v, bias_s);
             }
             kb += unit_ring_rows(ru.rows);
         }
-        if (!ok && lane == 0) {
-            if (!aborted) atomicOr(a.error, 1u);
-            aborted = 1;
-        }
+    }
+    if (!ok && lane == 0) {
+        if (!aborted) atomicOr(a.error, 1u);
+        aborted = 1;
     }
     __syncthreads();
     if (aborted && warp == kRowMmaWarp) mbar_wait(dbar, 0, kWaitNs);  // issued MMAs finish (bounded)
@@ -645,12 +694,203 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o
         // Let the issued copies land (bounded) before the CTA exits: the last
         // fill of each stage is its latest phase.
         for (int j = max(0, filled - kRowStages); j < filled; j++)
-            mbar_wait(sfull0 + 8 * (j % kRowStages), uint32_t((j / kRowStages) & 1), kWaitNs / 8);
+            mbar_wait(rb.sfull + 8 * (j % kRowStages), uint32_t((j / kRowStages) & 1), kWaitNs / 8);
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(C::TMEM_COLS));
+}
+
+// Two layers in one pass: layer A (CIN -> 32) feeds layer B (32 -> COUT)
+// through a ring of row stages in shared memory, so A's output never goes
+// to HBM. A's MMA warp and epilogue run the one-layer scheme over A's rows
+// (output rows sy0 - 1 .. sy0 + rows, the ones B reads); A's epilogue writes
+// each finished pair of rows, biased and rectified as bf16 chunks (zeros
+// outside the picture), into a stage of the ring, which B's MMA warp reads as
+// its input rows. A's strip is 128 pixels from sx0 - 1, so B's outputs are
+// exact for the 126 pixels from sx0 (lanes 126, 127 lack their right
+// neighbours and are not stored): strips are RM - 2 pixels apart.
+// Warps: 0-3 A's epilogue, 4-7 B's epilogue, the producer, A's MMA warp,
+// B's MMA warp. Two CTAs an SM (Ring2: each layer's ring takes 4 x 32
+// tensor-memory columns, and a CTA about 100 KB of shared memory), so that
+// one CTA's MMAs are issued while the other's warps wait.
+using Ring2 = Ring<4, 2>;
+constexpr int kFuseEpiA = 0, kFuseEpiB = 4, kFuseProducerWarp = 8, kFuseMmaA = 9, kFuseMmaB = 10;
+constexpr int kFuseThreads = 32 * (kFuseMmaB + 1);
+constexpr int kFuseStrip = RM - 2;
+
+template <int CIN, int COUT>
+struct FuseCfg {
+    using A = RowCfg<CIN, kHid>;
+    using B = RowCfg<kHid, COUT>;
+    static constexpr int WA = (A::W_BYTES + 127) & ~127, WB = (B::W_BYTES + 127) & ~127;
+    static constexpr int SMEM = WA + WB + Ring2::stages * (A::STAGE + B::STAGE);
+    static constexpr uint32_t TMEM_B = Ring2::slots * kHid;  // B's ring after A's
+    static constexpr uint32_t TMEM_COLS = 256;
+    static_assert(TMEM_B + Ring2::slots * COUT <= TMEM_COLS, "tensor memory");
+};
+
+template <int CIN, int COUT, int MODE>
+__global__ void __launch_bounds__(kFuseThreads, 2) k_sg_rows2(ConvArgs a, ConvArgs bl, RgbOut o, int strips, int segs,
+                                                              int seg_rows, int nunits) {
+    using F = FuseCfg<CIN, COUT>;
+    using LA = typename F::A;
+    using LB = typename F::B;
+    using R = Ring2;
+    constexpr int S = R::stages, Q = R::pairs;
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bars[4 * S + 4 * Q + 3];
+    __shared__ uint32_t tmem_slot;
+    __shared__ float bias_a[kHid], bias_b[COUT];
+    volatile __shared__ int aborted;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int first = blockIdx.x, stride = gridDim.x;
+    const int n = first < nunits ? (nunits - 1 - first) / stride + 1 : 0;  // this CTA's units
+    // A's weights, B's weights, A's input stages, the middle ring.
+    const uint32_t wa = smem_u32(smem), wb = wa + uint32_t(F::WA), sta = wb + uint32_t(F::WB),
+                   mid = sta + uint32_t(S * LA::STAGE);
+    auto bar = [&](int i) { return smem_u32(&bars[i]); };
+    const RowBars ra{bar(0), bar(S), bar(2 * S), bar(2 * S + Q)};
+    const RowBars rb{bar(2 * S + 2 * Q), bar(3 * S + 2 * Q), bar(4 * S + 2 * Q), bar(4 * S + 3 * Q)};
+    const uint32_t wbar = bar(4 * S + 4 * Q), dbar_a = wbar + 8, dbar_b = wbar + 16;
+    if (tid == 0) {
+        init_bars<R>(ra, 1);
+        init_bars<R>(rb, 4);  // the middle ring's stages: A's four epilogue warps
+        mbar_init(wbar, 1);
+        mbar_init(dbar_a, 1);
+        mbar_init(dbar_b, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        aborted = 0;
+    }
+    if (tid < kHid) bias_a[tid] = a.bias[tid];
+    if (tid < COUT) bias_b[tid] = bl.bias[tid];
+    // Middle-ring window columns 128 and 129 (right of A's 128 pixels) stay
+    // zero: they reach only B's lanes 126 and 127, which are not stored.
+    for (int z = tid; z < S * 2 * LB::C8 * 2; z += blockDim.x) {
+        const int c = z & 1, p = (z >> 1) % LB::C8, e = (z / (2 * LB::C8)) & 1, s = z / (4 * LB::C8);
+        st_shared_zero16(mid + uint32_t(s * LB::STAGE + e * LB::ROW + p * LB::PLANE + (RM + c) * 16));
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(F::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    int filled = 0;  // producer: stages filled
+    bool ok = true;
+
+    if (warp == kFuseProducerWarp) {
+        if (lane == 0) {
+            mbar_expect_tx(wbar, uint32_t(LA::W_BYTES + LB::W_BYTES));
+            bulk_copy(wa, a.w, uint32_t(LA::W_BYTES), wbar);
+            bulk_copy(wb, bl.w, uint32_t(LB::W_BYTES), wbar);
+        }
+        for (int u = 0; ok && u < n; u++) {
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, kFuseStrip, a.H);
+            ok = produce_span<CIN, R>(a, RowSpan{ru.img, ru.sx0 - 2, ru.sy0 - 2, ru.rows + 4}, sta, ra.sfull,
+                                      ra.sempty, filled, aborted, lane);
+        }
+    } else if (warp == kFuseMmaA || warp == kFuseMmaB) {
+        const bool is_a = warp == kFuseMmaA;
+        ok = __all_sync(0xFFFFFFFFu, mbar_wait(wbar, 0, kWaitNs));
+        int kb = 0, used = 0;
+        for (int u = 0; ok && u < n; u++) {
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, kFuseStrip, a.H);
+            ok = is_a ? mma_unit<CIN, kHid, R>(ru.rows + 2, ru.sy0 - 2, a.H, sta, LA::STAGE, ra, wa, tmem, kb, used,
+                                               aborted)
+                      : mma_unit<kHid, COUT, R>(ru.rows, ru.sy0 - 1, a.H, mid, LB::STAGE, rb, wb, tmem + F::TMEM_B, kb,
+                                                used, aborted);
+        }
+        umma_commit(is_a ? dbar_a : dbar_b);  // every issued MMA
+    } else if (warp < kFuseEpiB) {
+        // A's epilogue: pairs of A's output rows into the middle ring.
+        const int q = warp & 3, m = 32 * q + lane;
+        const uint32_t lanes = uint32_t(32 * q) << 16;
+        for (int ps = 0; ps < Q; ps++) pair_init<kHid>(ra, ps, tmem + lanes + uint32_t(2 * ps * kHid), lane);
+        int kb = 0;
+        for (int u = 0; ok && u < n; u++) {
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, kFuseStrip, a.H);
+            const int rows_a = ru.rows + 2, px = ru.sx0 - 1 + m;
+            for (int p = 0; 2 * p < rows_a; p++) {
+                const int P = kb / 2 + p, ms = P % S;
+                const uint32_t slot0 = tmem + lanes + uint32_t(2 * (P % Q) * kHid);
+                // The middle stage must have been read by B's MMAs (the first
+                // round passes: its parity refers to the phase before the
+                // barrier's first).
+                ok = __all_sync(0xFFFFFFFFu,
+                                !aborted && mbar_wait(rb.sempty + 8 * ms, uint32_t(((P / S) & 1) ^ 1), kWaitNs));
+                if (!ok) break;
+                uint32_t v[kHid];
+                if (!(ok = pair_first<kHid, R>(ra, P, slot0, v, aborted))) break;
+                const uint32_t dst = mid + uint32_t(ms * LB::STAGE + m * 16);
+#pragma unroll 1
+                for (int e = 0; e < 2; e++) {
+                    if (e == 1) pair_second<kHid, R>(ra, P, slot0 + uint32_t(kHid), v, lane);
+                    const int y = ru.sy0 - 1 + 2 * p + e;
+                    const bool keep = px >= 0 && px < a.W && y >= 0 && y < a.H && in_valid(a.valid, ru.img, px, y);
+#pragma unroll
+                    for (int c8 = 0; c8 < kHid / 8; c8++) {
+                        float f[8];
+#pragma unroll
+                        for (int k = 0; k < 8; k++) {
+                            const float s = __fadd_rn(__uint_as_float(v[c8 * 8 + k]), bias_a[c8 * 8 + k]);
+                            f[k] = keep ? fmaxf(s, 0.0f) : 0.0f;
+                        }
+                        asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(
+                                         dst + uint32_t(e * LB::ROW + c8 * LB::PLANE)),
+                                     "r"(pack_bf16x2(f[0], f[1])), "r"(pack_bf16x2(f[2], f[3])),
+                                     "r"(pack_bf16x2(f[4], f[5])), "r"(pack_bf16x2(f[6], f[7]))
+                                     : "memory");
+                    }
+                }
+                // B's MMAs read the stage through the async proxy.
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(rb.sfull + 8 * ms);
+            }
+            kb += unit_ring_rows(rows_a);
+        }
+    } else {
+        // B's epilogue: pairs of B's output rows to memory.
+        const int q = warp & 3, m = 32 * q + lane;
+        const uint32_t lanes = uint32_t(32 * q) << 16;
+        for (int ps = 0; ps < Q; ps++) pair_init<COUT>(rb, ps, tmem + F::TMEM_B + lanes + uint32_t(2 * ps * COUT), lane);
+        int kb = 0;
+        for (int u = 0; ok && u < n; u++) {
+            const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, kFuseStrip, a.H);
+            const int px = ru.sx0 + m;
+            const bool store = m < kFuseStrip && px < a.W;
+            for (int p = 0; 2 * p < ru.rows; p++) {
+                const int P = kb / 2 + p;
+                const uint32_t slot0 = tmem + F::TMEM_B + lanes + uint32_t(2 * (P % Q) * COUT);
+                uint32_t v[COUT];
+                if (!(ok = pair_first<COUT, R>(rb, P, slot0, v, aborted))) break;
+                if (store) store_pixel<COUT, MODE>(bl, o, ru.img, px, ru.sy0 + 2 * p, v, bias_b);
+                pair_second<COUT, R>(rb, P, slot0 + uint32_t(COUT), v, lane);
+                if (store && 2 * p + 1 < ru.rows) store_pixel<COUT, MODE>(bl, o, ru.img, px, ru.sy0 + 2 * p + 1, v, bias_b);
+            }
+            kb += unit_ring_rows(ru.rows);
+        }
+    }
+    if (!ok && lane == 0) {
+        if (!aborted) atomicOr(a.error, 1u);
+        aborted = 1;
+    }
+    __syncthreads();
+    if (aborted && (warp == kFuseMmaA || warp == kFuseMmaB))
+        mbar_wait(warp == kFuseMmaA ? dbar_a : dbar_b, 0, kWaitNs);  // issued MMAs finish (bounded)
+    if (aborted && tid == kFuseProducerWarp * 32) {
+        for (int j = max(0, filled - S); j < filled; j++)
+            mbar_wait(ra.sfull + 8 * (j % S), uint32_t((j / S) & 1), kWaitNs / 8);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(F::TMEM_COLS));
 }
 
 // cuTensorMapEncodeTiled, looked up once through the runtime (no link
@@ -671,17 +911,17 @@ EncodeTiledFn encode_tiled() {
     return fn;
 }
 
-// Rows per work unit: the run length whose units, spread over two CTAs an
-// SM, give the fewest input rows to the busiest CTA (a unit of S rows reads
-// S + 2; a CTA's rows follow one another through its pipeline, so a CTA, not
-// an SM, sets the pace).
-int row_segment(int strips, int H, int images, int sms) {
+// Rows per work unit: the run length whose units, spread over `ctas` CTAs,
+// give the fewest input rows to the busiest CTA (a unit of S rows reads
+// S + halo; a CTA's rows follow one another through its pipeline, so a CTA,
+// not an SM, sets the pace).
+int row_segment(int strips, int H, int images, long ctas, int halo) {
     int best = H;
     long best_cost = LONG_MAX;
     for (int S = 8;; S += 8) {
         const int rows = std::min(S, H), segs = (H + rows - 1) / rows;
         const long units = long(strips) * segs * images;
-        const long cost = (units + 2L * sms - 1) / (2L * sms) * (rows + 2);
+        const long cost = (units + ctas - 1) / ctas * (rows + halo);
         if (cost < best_cost) {
             best_cost = cost;
             best = rows;
@@ -691,6 +931,25 @@ int row_segment(int strips, int H, int images, int sms) {
     return best;
 }
 
+// The SM count of the current device, and the kernel's shared-memory limit
+// set once per device (kept per device in atomics: contexts on several
+// threads launch too).
+template <class K>
+cudaError_t kernel_setup(K kernel, int smem, std::atomic<int>* sms_of, int* sms) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    *sms = sms_of[dev].load(std::memory_order_acquire);
+    if (*sms == 0) {
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        sms_of[dev].store(*sms, std::memory_order_release);
+    }
+    return cudaSuccess;
+}
+
 template <int CIN, int COUT, int MODE>
 cudaError_t conv_launch(const ConvArgs& a, const RgbOut& o, int images, cudaStream_t s) {
     using C = RowCfg<CIN, COUT>;
@@ -698,28 +957,39 @@ cudaError_t conv_launch(const ConvArgs& a, const RgbOut& o, int images, cudaStre
     // CTAs share an SM (their accumulator rings fit in its 512 tensor-memory
     // columns; a third CTA's allocation would wait for one of them).
     constexpr int smem = std::max(((C::W_BYTES + 127) & ~127) + kRowStages * C::STAGE, 80 * 1024);
-    // The shared-memory limit and the SM count, set and read once per device
-    // (kept per device in atomics: contexts on several threads launch too).
     static std::atomic<int> sms_of[kMaxDevices];
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    int sms = 0;
+    const cudaError_t e = kernel_setup(k_sg_rows<CIN, COUT, MODE>, smem, sms_of, &sms);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    int sms = sms_of[dev].load(std::memory_order_acquire);
-    if (sms == 0) {
-        e = cudaFuncSetAttribute(k_sg_rows<CIN, COUT, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e != cudaSuccess) return e;
-        sms_of[dev].store(sms, std::memory_order_release);
-    }
     if (a.W <= 0 || a.H <= 0 || images <= 0) return cudaErrorInvalidValue;
     const int strips = (a.W + RM - 1) / RM;
-    const int seg_rows = row_segment(strips, a.H, images, sms);
+    const int seg_rows = row_segment(strips, a.H, images, 2L * sms, 2);
     const int segs = (a.H + seg_rows - 1) / seg_rows;
     const long nunits = long(strips) * segs * images;
     if (nunits > INT_MAX) return cudaErrorInvalidValue;
     const int grid = int(std::max(1L, std::min(nunits, 2L * sms)));
     k_sg_rows<CIN, COUT, MODE><<<grid, kRowThreads, smem, s>>>(a, o, strips, segs, seg_rows, int(nunits));
+    count_launch();
+    return cudaGetLastError();
+}
+
+// Layers A (a: CIN -> 32) and B (b: 32 -> COUT) in one pass.
+template <int CIN, int COUT, int MODE>
+cudaError_t conv2_launch(const ConvArgs& a, const ConvArgs& b, const RgbOut& o, int images, cudaStream_t s) {
+    constexpr int smem = FuseCfg<CIN, COUT>::SMEM;
+    static_assert(smem <= 227 * 1024, "shared memory");
+    static std::atomic<int> sms_of[kMaxDevices];
+    int sms = 0;
+    const cudaError_t e = kernel_setup(k_sg_rows2<CIN, COUT, MODE>, smem, sms_of, &sms);
+    if (e != cudaSuccess) return e;
+    if (a.W <= 0 || a.H <= 0 || images <= 0 || b.W != a.W || b.H != a.H) return cudaErrorInvalidValue;
+    const int strips = (a.W + kFuseStrip - 1) / kFuseStrip;
+    const int seg_rows = row_segment(strips, a.H, images, 2L * sms, 4);
+    const int segs = (a.H + seg_rows - 1) / seg_rows;
+    const long nunits = long(strips) * segs * images;
+    if (nunits > INT_MAX) return cudaErrorInvalidValue;
+    const int grid = int(std::max(1L, std::min(nunits, 2L * sms)));
+    k_sg_rows2<CIN, COUT, MODE><<<grid, kFuseThreads, smem, s>>>(a, b, o, strips, segs, seg_rows, int(nunits));
     count_launch();
     return cudaGetLastError();
 }
@@ -737,6 +1007,13 @@ struct PackArgs {
     uint4* in;      // [2][hq][wq] chunks
     float* base;    // [3][hq][wq]
     float* noise_minmax;  // optional: atomic min / max of the noise channel (as ordered ints)
+    // Optional (the develop's fallback): per 32x32 picture tile, a nonzero
+    // flag when a quad's noise channel leaves [fb_lo, fb_hi], and the count
+    // of such tiles.
+    unsigned* fb_flags;
+    unsigned* fb_count;
+    int tiles_x;
+    float fb_lo, fb_hi;
 };
 
 __device__ __forceinline__ float sg_nrm(const PackArgs& p, int x, int y) {
@@ -787,12 +1064,16 @@ __global__ void k_sg_pack(PackArgs p) {
     p.base[q] = r;
     p.base[plane + q] = gm;
     p.base[2 * plane + q] = b;
+    // The noise channel as the network sees it (bf16).
+    const float nb = bf16_lo(pack_bf16x2(noise, 0.0f));
     if (p.noise_minmax) {
-        // The noise channel as the network sees it (bf16), as a non-negative
-        // float whose bits order like ints.
-        const float nb = bf16_lo(pack_bf16x2(noise, 0.0f));
+        // As a non-negative float, its bits order like ints.
         atomicMin(reinterpret_cast<int*>(p.noise_minmax), __float_as_int(nb));
         atomicMax(reinterpret_cast<int*>(p.noise_minmax) + 1, __float_as_int(nb));
+    }
+    if (p.fb_flags && !(nb >= p.fb_lo && nb <= p.fb_hi)) {
+        const int tile = (sj / (kDevelopTile / 2)) * p.tiles_x + si / (kDevelopTile / 2);  // picture tile
+        if (atomicOr(p.fb_flags + tile, 1u) == 0) atomicAdd(p.fb_count, 1u);
     }
 }
 
@@ -817,25 +1098,6 @@ __global__ void k_sg_pack_weights(const float* __restrict__ params, uint16_t* __
     const int co = n % cout, ky = 2 - n / cout, ci = 16 * h + 8 * kc + e;
     const float wv = params[layer_off(l) + (size_t(co) * cin + ci) * 9 + ky * 3 + kx];
     packed[i] = __bfloat16_as_ushort(__float2bfloat16_rn(wv));
-}
-
-// Per 32x32 picture tile: does any quad's noise channel leave [lo, hi]?
-__global__ void k_sg_fallback(const uint4* __restrict__ in, int wq, int hq, int rr, int rc, int tiles_x, float lo,
-                              float hi, uint8_t* __restrict__ mask, unsigned* __restrict__ count) {
-    const int tile = blockIdx.x;
-    const int qx0 = (tile % tiles_x) * (kDevelopTile / 2), qy0 = (tile / tiles_x) * (kDevelopTile / 2);
-    const int u = threadIdx.x % 16, v = threadIdx.x / 16;
-    int out = 0;
-    if (qx0 + u < wq && qy0 + v < hq) {
-        const size_t q = size_t(mirror_q(qy0 + v, hq, rr)) * wq + mirror_q(qx0 + u, wq, rc);
-        const float n = bf16_lo(in[q].z);
-        out = (n < lo || n > hi) ? 1 : 0;
-    }
-    out = __syncthreads_or(out);
-    if (threadIdx.x == 0) {
-        mask[tile] = uint8_t(out);
-        if (out) atomicAdd(count, 1u);
-    }
 }
 
 // --- training ------------------------------------------------------------------------
@@ -1060,33 +1322,39 @@ struct NetBuffers {
 };
 
 // The seven layers; the head writes f32 channels (nb.head), or, given
-// `out`, the develop output directly.
+// `out`, the develop output directly. `fused` runs layers 0-1, 2-3 and 4-5
+// as pairs (k_sg_rows2: the first layer of a pair leaves no activations in
+// nb.act, so training, which reads them back, runs them one at a time).
 cudaError_t forward(const NetBuffers& nb, const uint16_t* packed, const float* params, const int4* valid, int images,
-                    int hq, int wq, unsigned* error, cudaStream_t s, const RgbOut* out = nullptr) {
+                    int hq, int wq, unsigned* error, cudaStream_t s, const RgbOut* out = nullptr, bool fused = false) {
     const RgbOut none{};
-    ConvArgs a{};
-    a.H = hq;
-    a.W = wq;
-    a.valid = valid;
-    a.error = error;
-    for (int l = 0; l < kLayers; l++) {
+    auto args = [&](int l) {
+        ConvArgs a{};
+        a.H = hq;
+        a.W = wq;
+        a.valid = valid;
+        a.error = error;
         a.x = l == 0 ? nb.in : nb.act[l - 1];
         a.w = reinterpret_cast<const uint4*>(packed + packed_off(l));
         a.bias = params + layer_off(l) + size_t(cout_of(l)) * cin_of(l) * 9;
+        a.y = l < kLayers - 1 ? nb.act[l] : nullptr;
+        a.yf = l < kLayers - 1 || out ? nullptr : nb.head;
+        return a;
+    };
+    for (int l = 0; l < kLayers; l++) {
         cudaError_t e;
-        if (l == 0) {
-            a.y = nb.act[0];
-            e = conv_launch<kIn, kHid, kHidden>(a, none, images, s);
+        if (fused && l < kLayers - 1) {
+            e = l == 0 ? conv2_launch<kIn, kHid, kHidden>(args(0), args(1), none, images, s)
+                       : conv2_launch<kHid, kHid, kHidden>(args(l), args(l + 1), none, images, s);
+            l++;
+        } else if (l == 0) {
+            e = conv_launch<kIn, kHid, kHidden>(args(l), none, images, s);
         } else if (l < kLayers - 1) {
-            a.y = nb.act[l];
-            e = conv_launch<kHid, kHid, kHidden>(a, none, images, s);
+            e = conv_launch<kHid, kHid, kHidden>(args(l), none, images, s);
         } else if (out) {
-            a.y = nullptr;
-            e = conv_launch<kHid, kHead, kHeadRgb>(a, *out, images, s);
+            e = conv_launch<kHid, kHead, kHeadRgb>(args(l), *out, images, s);
         } else {
-            a.y = nullptr;
-            a.yf = nb.head;
-            e = conv_launch<kHid, kHead, kHeadF32>(a, none, images, s);
+            e = conv_launch<kHid, kHead, kHeadF32>(args(l), none, images, s);
         }
         if (e != cudaSuccess) return e;
     }
@@ -1196,8 +1464,11 @@ int learned_state(prr_ctx* c, LearnedState** out) {
     return PRR_OK;
 }
 
-// Pack a decoded frame into the surrogate input and colours.
-int pack_frame(prr_ctx* c, const DevelopDesc& d, uint4* in, float* base, float* minmax) {
+// Pack a decoded frame into the surrogate input and colours; optionally
+// the noise channel's range (training) or the fallback tiles of a model
+// (fb_flags zeroed beforehand: flags per 32x32 tile, count in fb_count).
+int pack_frame(prr_ctx* c, const DevelopDesc& d, uint4* in, float* base, float* minmax, unsigned* fb_flags = nullptr,
+               unsigned* fb_count = nullptr, float fb_lo = 0.0f, float fb_hi = 0.0f) {
     sg::PackArgs p{};
     p.codes = d.codes;
     p.stride = d.stride;
@@ -1222,6 +1493,11 @@ int pack_frame(prr_ctx* c, const DevelopDesc& d, uint4* in, float* base, float* 
     p.in = in;
     p.base = base;
     p.noise_minmax = minmax;
+    p.fb_flags = fb_flags;
+    p.fb_count = fb_count;
+    p.tiles_x = (d.w + kDevelopTile - 1) / kDevelopTile;
+    p.fb_lo = fb_lo;
+    p.fb_hi = fb_hi;
     dim3 grid((p.wq + 127) / 128, p.hq);
     sg::k_sg_pack<<<grid, 128, 0, c->stream>>>(p);
     count_launch();
@@ -1249,11 +1525,11 @@ int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* param
     const size_t plane = size_t(wq) * hq;
     const int tiles_x = (d.w + kDevelopTile - 1) / kDevelopTile, tiles_y = (d.h + kDevelopTile - 1) / kDevelopTile;
     const size_t ntiles = size_t(tiles_x) * tiles_y;
-    // Scratch: input chunks, colours, two activation buffers, mask (the head
-    // writes the output planes itself).
+    // Scratch: input chunks, colours, two activation buffers, fallback
+    // flags per tile (the head writes the output planes itself).
     const size_t o_in = 0, o_base = o_in + up256(plane * 32), o_a0 = o_base + up256(plane * 12),
                  o_a1 = o_a0 + up256(plane * 64), o_mask = o_a1 + up256(plane * 64),
-                 total = o_mask + up256(ntiles);
+                 total = o_mask + up256(ntiles * sizeof(unsigned));
     PRR_TRY(c->cuda(L->scratch.ensure(total)));
     PRR_TRY(c->cuda(L->packed.ensure(sg::kPacked)));
     PRR_TRY(c->cuda(L->counters.ensure(2)));
@@ -1264,16 +1540,18 @@ int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* param
     float* base = reinterpret_cast<float*>(S + o_base);
     uint4* a0 = reinterpret_cast<uint4*>(S + o_a0);
     uint4* a1 = reinterpret_cast<uint4*>(S + o_a1);
-    for (int l = 0; l < 6; l++) nb.act[l] = (l & 1) ? a1 : a0;
+    // The fused forward writes act[1], act[3], act[5] (each pair's second
+    // layer) and reads the one before: they alternate between the buffers.
+    for (int l = 0; l < 6; l++) nb.act[l] = ((l >> 1) & 1) ? a1 : a0;
     nb.head = nullptr;
-    uint8_t* mask = S + o_mask;
+    unsigned* mask = reinterpret_cast<unsigned*>(S + o_mask);
     cudaStream_t s = c->stream;
     PRR_TRY(c->cuda(cudaMemsetAsync(L->counters.p, 0, 2 * sizeof(unsigned), s)));
-    PRR_TRY(pack_frame(c, d, nb.in, base, nullptr));
+    PRR_TRY(c->cuda(cudaMemsetAsync(mask, 0, ntiles * sizeof(unsigned), s)));
+    // The packing flags the tiles whose noise channel leaves the model's
+    // range: the plain develop takes those.
+    PRR_TRY(pack_frame(c, d, nb.in, base, nullptr, mask, L->counters.p, model->noise_lo, model->noise_hi));
     PRR_TRY(c->cuda(sg::pack_weights(model->dev_params, L->packed.p, s)));
-    sg::k_sg_fallback<<<unsigned(ntiles), 256, 0, s>>>(nb.in, wq, hq, d.cfa >> 1, d.cfa & 1, tiles_x, model->noise_lo,
-                                                       model->noise_hi, mask, L->counters.p);
-    count_launch();
     sg::RgbOut o{};
     o.base = base;
     o.w = d.w;
@@ -1288,7 +1566,7 @@ int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* param
     o.b = b;
     o.fallback = mask;
     o.tiles_x = tiles_x;
-    PRR_TRY(c->cuda(sg::forward(nb, L->packed.p, model->dev_params, nullptr, 1, hq, wq, L->counters.p + 1, s, &o)));
+    PRR_TRY(c->cuda(sg::forward(nb, L->packed.p, model->dev_params, nullptr, 1, hq, wq, L->counters.p + 1, s, &o, true)));
     PRR_TRY(c->cuda(cudaGetLastError()));
     // The plain develop on the fallback tiles (the others return at once).
     d.tile_mask = mask;

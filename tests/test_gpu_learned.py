@@ -113,6 +113,28 @@ def test_network_free_output_is_exact(pattern, stage):
     assert np.array_equal(got.reshape(3, 132, 200), want)
 
 
+# The develop runs layers 0-1, 2-3 and 4-5 as fused pairs (strips of 126
+# pixels): its output against the oracle's network and output stage, on
+# frames of several strips and both mirrorings of the network frame.
+@pytest.mark.parametrize("w,h,pattern", [(560, 300, 0), (506, 138, 3), (66, 40, 1)])
+def test_develop_output_matches_the_oracle(w, h, pattern):
+    pkt = encoded_frame(w, h, pattern, seed=9, sigma=12.0, qscale=25)
+    frame = P.decode_frame(pkt)
+    rng = np.random.default_rng(w + h)
+    params = he_params(rng, 0.5)
+    got, nfb = planes_of(frame, P.Stage.REC2020, Lrn.Surrogate(params, 0.0, float("inf")))
+    assert nfb == 0
+    of = O.decode_frame(pkt)
+    p = O.params_new(of.header, of.quantizer)
+    in16, base = O.sg_pack(of.header, of.samples, p)
+    _, head = O.sg_forward(in16, params)
+    want = O.sg_output(head, base, w, h, O.output_matrix(of.header), cfa=p.cfa_phase)
+    scale = max(1.0, float(np.max(np.abs(head))))
+    err = np.abs(got.reshape(3, h, w) - want)
+    assert float(np.max(err)) <= 4e-2 * scale, float(np.max(err))
+    assert float(np.mean(err)) <= 2e-3 * scale, float(np.mean(err))
+
+
 def test_fallback_tiles_are_the_plain_develop():
     pkt = encoded_frame(256, 160, 0, seed=7, sigma=16.0, qscale=30)
     frame = P.decode_frame(pkt)
