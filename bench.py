@@ -1315,7 +1315,7 @@ def run_learned(args):
         return el
 
     e2e_run(2 * nthreads)
-    e2e_n = max(4 * nthreads, args.steps // 4)
+    e2e_n = max(4 * nthreads, args.steps)
     e2e_s = R.reduce_max(e2e_run(e2e_n))
     if rank == 0:
         peak, pk = tensor_peak()
