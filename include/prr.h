@@ -343,6 +343,14 @@ int prr_develop_learned(prr_ctx* ctx, const prr_header* header, const prr_params
                         const uint16_t* dev_samples, const prr_sg_model* model, int layout, float* r,
                         float* g, float* b, size_t out_len, uint32_t* fallback_tiles);
 
+/* Diagnostic: the network input and quad colours prr_develop_learned packs
+ * from a decoded frame (stage as there), into host buffers: in16
+ * [16][hq][wq] (the bf16 channels widened to f32) and base3 [3][hq][wq]
+ * (red, mean green, blue), hq x wq = the frame's quads, network frame (the
+ * picture mirrored so that red sits top left). Waits for the device. */
+int prr_sg_pack(prr_ctx* ctx, const prr_header* header, const prr_params* params, int stage,
+                const uint16_t* dev_samples, float* in16, float* base3);
+
 /* Training on the device with the library's own forward (tensor cores) and
  * backward (f32) kernels and Adam. Frames are added decoded; their plain
  * white-balanced develop is the target. A step trains on `batch` crops of

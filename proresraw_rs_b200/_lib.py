@@ -306,6 +306,7 @@ def lib():
         "prr_sg_trainer_get_params": (i, [vp, vp]),
         "prr_sg_trainer_device_params": (vp, [vp]),
         "prr_sg_trainer_step": (i, [vp, vp, C.c_float, P(C.c_float)]),
+        "prr_sg_pack": (i, [vp, P(CHeader), P(CParams), i, vp, vp, vp]),
         "prr_sg_gradients": (i, [vp, vp, vp, vp, C.c_uint32, C.c_uint32, vp, vp, vp, P(C.c_double)]),
         "prr_mov_open": (i, [C.c_char_p, MOV_ACCEPT_FN, vp, P(vp), C.c_char_p, sz]),
         "prr_mov_close": (None, [vp]),

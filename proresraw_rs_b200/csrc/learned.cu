@@ -1037,23 +1037,48 @@ __device__ __forceinline__ float sg_green(const PackArgs& p, int i, int j) {
 // the bottom row, so that every Bayer pattern reaches the network as RGGB.
 __host__ __device__ __forceinline__ int mirror_q(int i, int n, int flip) { return flip ? n - 1 - i : i; }
 
-__global__ void k_sg_pack(PackArgs p) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (i >= p.wq) return;
-    const int si = mirror_q(i, p.wq, p.rc), sj = mirror_q(j, p.hq, p.rr);  // picture quad
-    const int ex = p.rc ? -1 : 1, sy = p.rr ? -1 : 1;                     // network east / south
+// A CTA packs a tile of kPackW x kPackH network-frame quads. Each quad's
+// mean green is computed once into shared memory, with a one-quad halo
+// (clamped at the picture's edges as sg_green clamps), for the neighbours'
+// gradients and Laplacian.
+constexpr int kPackW = 32, kPackH = 8;
+
+__global__ void __launch_bounds__(kPackW * kPackH) k_sg_pack(PackArgs p) {
+    __shared__ float gms[kPackH + 2][kPackW + 2];
+    const int tx = threadIdx.x % kPackW, ty = threadIdx.x / kPackW;
+    const int i0 = blockIdx.x * kPackW, j0 = blockIdx.y * kPackH;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool inside = i < p.wq && j < p.hq;
+    // Network-frame quad (i, j) is picture quad (si, sj).
+    const int si = mirror_q(min(i, p.wq - 1), p.wq, p.rc), sj = mirror_q(min(j, p.hq - 1), p.hq, p.rr);
     const int x0 = 2 * si, y0 = 2 * sj;
-    const float r = __fmul_rn(sg_nrm(p, x0 + p.rc, y0 + p.rr), p.wb0);
     const float gr = sg_nrm(p, x0 + 1 - p.rc, y0 + p.rr);
     const float gb = sg_nrm(p, x0 + p.rc, y0 + 1 - p.rr);
-    const float b = __fmul_rn(sg_nrm(p, x0 + 1 - p.rc, y0 + 1 - p.rr), p.wb1);
     const float gm = __fmul_rn(__fadd_rn(gr, gb), 0.5f);
+    gms[ty + 1][tx + 1] = gm;  // a quad past the picture's edge: its clamped neighbour, as sg_green
+    // The halo ring: 2 (kPackW + 2) + 2 kPackH cells.
+    for (int c = threadIdx.x; c < 2 * (kPackW + 2) + 2 * kPackH; c += blockDim.x) {
+        int cx, cy;
+        if (c < 2 * (kPackW + 2)) {
+            cx = c % (kPackW + 2);
+            cy = c < kPackW + 2 ? 0 : kPackH + 1;
+        } else {
+            const int k = c - 2 * (kPackW + 2);
+            cx = (k & 1) ? kPackW + 1 : 0;
+            cy = 1 + (k >> 1);
+        }
+        gms[cy][cx] = sg_green(p, mirror_q(i0 - 1 + cx, p.wq, p.rc), mirror_q(j0 - 1 + cy, p.hq, p.rr));
+    }
+    __syncthreads();
+    if (!inside) return;
+    const float r = __fmul_rn(sg_nrm(p, x0 + p.rc, y0 + p.rr), p.wb0);
+    const float b = __fmul_rn(sg_nrm(p, x0 + 1 - p.rc, y0 + 1 - p.rr), p.wb1);
     const float t = __fadd_rn(p.bs, gm);
     const float var = __fadd_rn(p.n2, fmaxf(p.n1, __fmul_rn(p.n0, __fmul_rn(t, t))));
     const float noise = __fmul_rn(64.0f, __fsqrt_rn(var));
-    const float ge = sg_green(p, si + ex, sj), gw = sg_green(p, si - ex, sj);
-    const float gs = sg_green(p, si, sj + sy), gn = sg_green(p, si, sj - sy);
+    // Network east / west / south / north neighbours.
+    const float ge = gms[ty + 1][tx + 2], gw = gms[ty + 1][tx];
+    const float gs = gms[ty + 2][tx + 1], gn = gms[ty][tx + 1];
     const float gx = __fmul_rn(__fsub_rn(ge, gw), 0.5f), gy = __fmul_rn(__fsub_rn(gs, gn), 0.5f);
     const float lap = __fsub_rn(gm, __fmul_rn(__fadd_rn(__fadd_rn(ge, gw), __fadd_rn(gs, gn)), 0.25f));
     auto d4 = [](float v, float ref) { return __fmul_rn(__fsub_rn(v, ref), 4.0f); };
@@ -1498,8 +1523,8 @@ int pack_frame(prr_ctx* c, const DevelopDesc& d, uint4* in, float* base, float* 
     p.tiles_x = (d.w + kDevelopTile - 1) / kDevelopTile;
     p.fb_lo = fb_lo;
     p.fb_hi = fb_hi;
-    dim3 grid((p.wq + 127) / 128, p.hq);
-    sg::k_sg_pack<<<grid, 128, 0, c->stream>>>(p);
+    dim3 grid((p.wq + sg::kPackW - 1) / sg::kPackW, (p.hq + sg::kPackH - 1) / sg::kPackH);
+    sg::k_sg_pack<<<grid, sg::kPackW * sg::kPackH, 0, c->stream>>>(p);
     count_launch();
     return c->cuda(cudaGetLastError());
 }
@@ -1511,6 +1536,55 @@ size_t up256(size_t v) { return (v + 255) & ~size_t(255); }
 extern "C" {
 
 size_t prr_sg_param_count(void) { return sg::kParams; }
+
+int prr_sg_pack(prr_ctx* c, const prr_header* h, const prr_params* params, int stage, const uint16_t* dev_samples,
+                float* in16, float* base3) {
+    if (!c || !h || !in16 || !base3) return PRR_ERR_INVALID;
+    PRR_TRY(c->use_device());
+    const int wq = (int(h->width) + 1) / 2, hq = (int(h->height) + 1) / 2;
+    const size_t plane = size_t(wq) * hq, n = size_t(h->width) * h->height;
+    DevBuf<uint4> in;
+    DevBuf<float> base;
+    HostBuf<uint4> hin;
+    auto cleanup = [&]() {
+        in.release();
+        base.release();
+        hin.release();
+    };
+    cudaError_t e = in.ensure(2 * plane);
+    if (e == cudaSuccess) e = base.ensure(3 * plane);
+    if (e == cudaSuccess) e = hin.ensure(2 * plane);
+    if (e != cudaSuccess) {
+        cleanup();
+        return c->cuda(e);
+    }
+    // The packing reads no output buffer: the input buffer stands in for the
+    // interleaved output the descriptor checks (aligned, never written).
+    DevelopDesc d{};
+    int rc = build_develop_desc(h, params, stage, dev_samples, PRR_INTERLEAVED, reinterpret_cast<float*>(in.p), nullptr,
+                                nullptr, 3 * n, &d);
+    if (rc == PRR_OK) rc = pack_frame(c, d, in.p, base.p, nullptr);
+    if (rc == PRR_OK) {
+        e = cudaMemcpyAsync(hin.p, in.p, 2 * plane * sizeof(uint4), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(base3, base.p, 3 * plane * sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        rc = c->cuda(e);
+    }
+    if (rc == PRR_OK) {
+        // Chunk k of quad q holds channels 8k .. 8k + 7 as bf16 pairs.
+        for (size_t q = 0; q < plane; q++)
+            for (int k = 0; k < 2; k++) {
+                const uint4 v = hin.p[k * plane + q];
+                const uint32_t words[4] = {v.x, v.y, v.z, v.w};
+                for (int ch = 0; ch < 8; ch++) {
+                    const uint32_t bits = (ch & 1) ? (words[ch >> 1] & 0xFFFF0000u) : (words[ch >> 1] << 16);
+                    std::memcpy(in16 + (size_t(8 * k + ch) * plane + q), &bits, 4);
+                }
+            }
+    }
+    cleanup();
+    return rc;
+}
 
 int prr_develop_learned(prr_ctx* c, const prr_header* h, const prr_params* params, int stage,
                         const uint16_t* dev_samples, const prr_sg_model* model, int layout, float* r, float* g,

@@ -118,6 +118,21 @@ def develop_learned(frame: Frame, stage: Stage, surrogate: Surrogate,
     return RgbPlanes(frame.header.width, frame.header.height, [r, g, b]), nfb
 
 
+def pack(frame: Frame, stage: Stage, params: Optional[DemosaicParams] = None) -> Tuple[np.ndarray, np.ndarray]:
+    """prr_sg_pack: the network input [16][hq][wq] and the quad colours
+    [3][hq][wq] the learned develop computes for a decoded frame (checking)."""
+    if params is None:
+        params = DemosaicParams.new(frame.header, frame.quantizer())
+    hq, wq = (frame.header.height + 1) // 2, (frame.header.width + 1) // 2
+    in16 = np.zeros((16, hq, wq), dtype=np.float32)
+    base = np.zeros((3, hq, wq), dtype=np.float32)
+    ctx = context()
+    rc = _lib.lib().prr_sg_pack(ctx, C.byref(frame.header._c), C.byref(params._c()), int(stage),
+                                _dptr(frame.samples), in16.ctypes.data, base.ctypes.data)
+    _check(rc, ctx=ctx)
+    return in16, base
+
+
 def gradients(in16: np.ndarray, base3: np.ndarray, target3: np.ndarray, params: np.ndarray):
     """Device forward, loss and gradient for one explicit image (checking)."""
     hq, wq = in16.shape[1:]

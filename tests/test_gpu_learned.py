@@ -94,6 +94,19 @@ def plain_of(frame, stage):
     return np.stack([p.cpu().numpy() for p in img.planes])
 
 
+@pytest.mark.parametrize("w,h", [(200, 132), (258, 70), (66, 18)])
+@pytest.mark.parametrize("pattern", [0, 1, 2, 3])
+def test_packing_is_exact(w, h, pattern):
+    # The network input (bf16 channels) and the quad colours, bit for bit.
+    pkt = encoded_frame(w, h, pattern, seed=3 + pattern, sigma=14.0, qscale=25)
+    frame = P.decode_frame(pkt)
+    in16, base = Lrn.pack(frame, P.Stage.REC2020)
+    of = O.decode_frame(pkt)
+    want_in, want_base = O.sg_pack(of.header, of.samples, O.params_new(of.header, of.quantizer))
+    assert np.array_equal(in16.view(np.uint32), want_in.view(np.uint32))
+    assert np.array_equal(base.view(np.uint32), want_base.view(np.uint32))
+
+
 @pytest.mark.parametrize("pattern", [0, 3])
 @pytest.mark.parametrize("stage", [P.Stage.WHITE_BALANCED, P.Stage.REC2020])
 def test_network_free_output_is_exact(pattern, stage):
