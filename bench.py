@@ -1336,9 +1336,11 @@ def run_learned(args):
                        "psnr_db_vs_plain": {"min": min(psnrs), "mean": float(np.mean(psnrs)), "max": max(psnrs)},
                        "max_abs_vs_plain": max(maxabs),
                        "fallback_tiles": fb, "fallback_rate": fb / tiles,
-                       "l2": "outputs (106 MB planes) and activations (141 MB per layer) exceed L2",
+                       "l2": "outputs (106 MB planes) and activations (141 MB in and out of each fused pair of "
+                             "layers) exceed L2",
                        "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "tensor", "kernel": "learned develop (7 conv launches + pack/output)",
+            "roofline": {"bound": "tensor",
+                         "kernel": "learned develop (three fused pairs of conv layers, the head, packing)",
                          "achieved": flops / (ms_l / 1000.0) / 1e12, "peak": peak, "unit": "TFLOP/s",
                          "frac": flops / (ms_l / 1000.0) / 1e12 / peak, "traffic": None, "peak_source": pk,
                          "flops_counted": "algorithmic: the network as specified (5 input channels, 12-wide head)",
