@@ -609,7 +609,7 @@ __device__ __forceinline__ void init_bars(const RowBars& b, uint32_t full_count)
     }
 }
 
-// One layer: a CTA per pair of SMs' halves (two an SM), the roles above.
+// One layer (k_sg_rows): persistent CTAs, two an SM, in the roles above.
 template <int CIN, int COUT, int MODE>
 __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o, int strips, int segs, int seg_rows,
                                                              int nunits) {
@@ -716,7 +716,7 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o
 // tensor-memory columns, and a CTA about 100 KB of shared memory), so that
 // one CTA's MMAs are issued while the other's warps wait.
 using Ring2 = Ring<4, 2>;
-constexpr int kFuseEpiA = 0, kFuseEpiB = 4, kFuseProducerWarp = 8, kFuseMmaA = 9, kFuseMmaB = 10;
+constexpr int kFuseEpiB = 4, kFuseProducerWarp = 8, kFuseMmaA = 9, kFuseMmaB = 10;  // A's epilogue: warps 0-3
 constexpr int kFuseThreads = 32 * (kFuseMmaB + 1);
 constexpr int kFuseStrip = RM - 2;
 
