@@ -148,6 +148,37 @@ def test_develop_output_matches_the_oracle(w, h, pattern):
     assert float(np.mean(err)) <= 2e-3 * scale, float(np.mean(err))
 
 
+def test_interleaved_output_is_the_planar_output():
+    # prr_develop_learned with PRR_INTERLEAVED (rgb per pixel) against the
+    # planar call, on a frame with some fallback tiles.
+    import ctypes as C
+    import torch
+    from proresraw_rs_b200 import _lib, _dptr, context
+    pkt = encoded_frame(300, 200, 3, seed=8, sigma=18.0, qscale=30)
+    frame = P.decode_frame(pkt)
+    rng = np.random.default_rng(8)
+    params = he_params(rng, 0.5)
+    of = O.decode_frame(pkt)
+    noise = O.sg_pack(of.header, of.samples, O.params_new(of.header, of.quantizer))[0][4]
+    s = Lrn.Surrogate(params, 0.0, float(np.median(noise)))
+    planar, nfb = planes_of(frame, P.Stage.REC2020, s)
+    assert nfb > 0
+    n = 300 * 200
+    out = torch.empty(3 * n, dtype=torch.float32, device="cuda")
+    prm = P.DemosaicParams.new(frame.header, frame.quantizer())
+    dp = s.device()
+    ctx = context()
+    m = Lrn._model(s, dp)
+    nfb2 = C.c_uint32()
+    rc = _lib.lib().prr_develop_learned(ctx, C.byref(frame.header._c), C.byref(prm._c()), int(P.Stage.REC2020),
+                                        _dptr(frame.samples), C.byref(m), 0, _dptr(out), None, None, 3 * n,
+                                        C.byref(nfb2))
+    assert rc == 0
+    assert nfb2.value == nfb
+    inter = out.cpu().numpy().reshape(n, 3).T
+    assert np.array_equal(inter, planar.reshape(3, n))
+
+
 def test_fallback_tiles_are_the_plain_develop():
     pkt = encoded_frame(256, 160, 0, seed=7, sigma=16.0, qscale=30)
     frame = P.decode_frame(pkt)
