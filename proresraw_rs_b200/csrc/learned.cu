@@ -92,9 +92,14 @@ template <int SLOTS, int STAGES>
 struct Ring {
     static constexpr int slots = SLOTS, pairs = SLOTS / 2, stages = STAGES;
 };
-using Ring1 = Ring<8, 4>;  // one layer a CTA, two CTAs an SM
-constexpr int kRowSlots = Ring1::slots, kRowPairs = Ring1::pairs, kRowStages = Ring1::stages;
-constexpr int kRowEpiWarps = 4 * kRowPairs;  // an epilogue group of four warps (128 lanes) per pair
+// One layer a CTA, two CTAs an SM: 256 tensor-memory columns a ring, so 8
+// rows of 32 channels or 16 rows of 16 (the head; a longer ring splits the
+// MMAs of fewer rows at its end).
+template <int COUT>
+using Ring1 = Ring<256 / COUT, 4>;
+constexpr int kRowStages = 4;
+constexpr int kRowGroups = 4;                 // epilogue groups of four warps (128 lanes)
+constexpr int kRowEpiWarps = 4 * kRowGroups;
 constexpr int kRowProducerWarp = kRowEpiWarps, kRowMmaWarp = kRowEpiWarps + 1;
 constexpr int kRowThreads = 32 * (kRowEpiWarps + 2);
 
@@ -120,7 +125,7 @@ struct RowCfg : RowIn<CIN> {
     using RowIn<CIN>::H2;
     static constexpr int NB = 3 * COUT;                // N of a full MMA: the three kernel rows stacked
     static constexpr int W_BYTES = 3 * H2 * 2 * NB * 16;  // = 9 x CIN x COUT bf16
-    static constexpr uint32_t TMEM_COLS = kRowSlots * COUT;  // one layer a CTA (Ring1)
+    static constexpr uint32_t TMEM_COLS = Ring1<COUT>::slots * COUT;  // one layer a CTA
     static_assert(CIN % 16 == 0 && COUT % 16 == 0 && NB <= 256, "tcgen05 shape");
     static_assert(TMEM_COLS >= 32 && (TMEM_COLS & (TMEM_COLS - 1)) == 0, "tensor memory allocation");
 };
@@ -614,8 +619,11 @@ template <int CIN, int COUT, int MODE>
 __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o, int strips, int segs, int seg_rows,
                                                              int nunits) {
     using C = RowCfg<CIN, COUT>;
+    using R = Ring1<COUT>;
+    constexpr int S = R::stages, Q = R::pairs;
+    static_assert(Q % kRowGroups == 0, "a pair slot belongs to one epilogue group");
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bars[2 * kRowStages + 2 * kRowPairs + 2];
+    __shared__ __align__(8) uint64_t bars[2 * S + 2 * Q + 2];
     __shared__ uint32_t tmem_slot;
     __shared__ float bias_s[COUT];
     volatile __shared__ int aborted;
@@ -626,10 +634,10 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o
     const uint32_t wsm = smem_u32(smem);
     const uint32_t st0 = wsm + uint32_t((C::W_BYTES + 127) & ~127);
     auto bar = [&](int i) { return smem_u32(&bars[i]); };
-    const RowBars rb{bar(0), bar(kRowStages), bar(2 * kRowStages), bar(2 * kRowStages + kRowPairs)};
-    const uint32_t wbar = bar(2 * kRowStages + 2 * kRowPairs), dbar = wbar + 8;
+    const RowBars rb{bar(0), bar(S), bar(2 * S), bar(2 * S + Q)};
+    const uint32_t wbar = bar(2 * S + 2 * Q), dbar = wbar + 8;
     if (tid == 0) {
-        init_bars<Ring1>(rb, 1);
+        init_bars<R>(rb, 1);
         mbar_init(wbar, 1);
         mbar_init(dbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -655,30 +663,32 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o
         }
         for (int u = 0; ok && u < n; u++) {
             const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, RM, a.H);
-            ok = produce_span<CIN, Ring1>(a, RowSpan{ru.img, ru.sx0 - 1, ru.sy0 - 1, ru.rows + 2}, st0, rb.sfull, rb.sempty,
-                                   filled, aborted, lane);
+            ok = produce_span<CIN, R>(a, RowSpan{ru.img, ru.sx0 - 1, ru.sy0 - 1, ru.rows + 2}, st0, rb.sfull, rb.sempty,
+                                      filled, aborted, lane);
         }
     } else if (warp == kRowMmaWarp) {
         ok = __all_sync(0xFFFFFFFFu, mbar_wait(wbar, 0, kWaitNs));
         int kb = 0, used = 0;  // ring rows of the earlier units; stages consumed
         for (int u = 0; ok && u < n; u++) {
             const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, RM, a.H);
-            ok = mma_unit<CIN, COUT, Ring1>(ru.rows, ru.sy0 - 1, a.H, st0, C::STAGE, rb, wsm, tmem, kb, used, aborted);
+            ok = mma_unit<CIN, COUT, R>(ru.rows, ru.sy0 - 1, a.H, st0, C::STAGE, rb, wsm, tmem, kb, used, aborted);
         }
         umma_commit(dbar);  // every issued MMA
     } else {
-        const int g = warp >> 2, q = warp & 3;  // group = pair slot; lane quarter
-        const uint32_t slot0 = tmem + (uint32_t(32 * q) << 16) + uint32_t(2 * g * COUT), slot1 = slot0 + uint32_t(COUT);
-        pair_init<COUT>(rb, g, slot0, lane);
+        const int g = warp >> 2, q = warp & 3;  // group (pair slots g, g + kRowGroups, ...); lane quarter
+        const uint32_t lanes = uint32_t(32 * q) << 16;
+        for (int ps = g; ps < Q; ps += kRowGroups) pair_init<COUT>(rb, ps, tmem + lanes + uint32_t(2 * ps * COUT), lane);
         int kb = 0;
         for (int u = 0; ok && u < n; u++) {
             const RowUnit ru = row_unit(first + u * stride, strips, segs, seg_rows, RM, a.H);
             const int px = ru.sx0 + 32 * q + lane;
-            for (int p = ((g - kb / 2) % kRowPairs + kRowPairs) % kRowPairs; 2 * p < ru.rows; p += kRowPairs) {
+            for (int p = ((g - kb / 2) % kRowGroups + kRowGroups) % kRowGroups; 2 * p < ru.rows; p += kRowGroups) {
+                const int P = kb / 2 + p;
+                const uint32_t slot0 = tmem + lanes + uint32_t(2 * (P % Q) * COUT);
                 uint32_t v[COUT];
-                if (!(ok = pair_first<COUT, Ring1>(rb, kb / 2 + p, slot0, v, aborted))) break;
+                if (!(ok = pair_first<COUT, R>(rb, P, slot0, v, aborted))) break;
                 if (px < a.W) store_pixel<COUT, MODE>(a, o, ru.img, px, ru.sy0 + 2 * p, v, bias_s);
-                pair_second<COUT, Ring1>(rb, kb / 2 + p, slot1, v, lane);
+                pair_second<COUT, R>(rb, P, slot0 + uint32_t(COUT), v, lane);
                 if (px < a.W && 2 * p + 1 < ru.rows) store_pixel<COUT, MODE>(a, o, ru.img, px, ru.sy0 + 2 * p + 1, v, bias_s);
             }
             kb += unit_ring_rows(ru.rows);
@@ -693,8 +703,8 @@ __global__ void __launch_bounds__(kRowThreads, 2) k_sg_rows(ConvArgs a, RgbOut o
     if (aborted && tid == kRowProducerWarp * 32) {
         // Let the issued copies land (bounded) before the CTA exits: the last
         // fill of each stage is its latest phase.
-        for (int j = max(0, filled - kRowStages); j < filled; j++)
-            mbar_wait(rb.sfull + 8 * (j % kRowStages), uint32_t((j / kRowStages) & 1), kWaitNs / 8);
+        for (int j = max(0, filled - S); j < filled; j++)
+            mbar_wait(rb.sfull + 8 * (j % S), uint32_t((j / S) & 1), kWaitNs / 8);
     }
     tc_fence_before();
     __syncthreads();
