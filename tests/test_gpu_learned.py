@@ -129,7 +129,7 @@ def test_network_free_output_is_exact(pattern, stage):
 # The develop runs layers 0-1, 2-3 and 4-5 as fused pairs (strips of 126
 # pixels): its output against the oracle's network and output stage, on
 # frames of several strips and both mirrorings of the network frame.
-@pytest.mark.parametrize("w,h,pattern", [(560, 300, 0), (506, 138, 3), (66, 40, 1)])
+@pytest.mark.parametrize("w,h,pattern", [(560, 300, 0), (506, 138, 3), (66, 40, 1), (66, 18, 2)])
 def test_develop_output_matches_the_oracle(w, h, pattern):
     pkt = encoded_frame(w, h, pattern, seed=9, sigma=12.0, qscale=25)
     frame = P.decode_frame(pkt)
